@@ -1,1 +1,22 @@
-"""prrtc_b200 package (stub)."""
+"""prrtc_b200 -- B200-native (sm_100a) pRRTC motion planner.
+
+Drop-in for P-RRAX's ``prrtc_plan`` path: the same API and collision_context
+contract, computed by hand-written CUDA kernels in ``libprrtc_b200.so``.
+"""
+from .prrtc import (  # noqa: F401
+    PRRTCResult,
+    lpt_order,
+    prrtc_extend,
+    prrtc_nearest_neighbor,
+    prrtc_plan,
+    prrtc_plan_batch,
+)
+
+__all__ = [
+    "PRRTCResult",
+    "prrtc_plan",
+    "prrtc_plan_batch",
+    "prrtc_nearest_neighbor",
+    "prrtc_extend",
+    "lpt_order",
+]

@@ -1,0 +1,92 @@
+// kernels.h -- host-side launch interface between the C-ABI layer (capi.cu) and
+// the kernel translation units.  Internal: not part of the public C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace prrtc {
+
+// Sources of the packed scene of every problem in a launch.  Robot tables are
+// shared; world tables are either shared (count pointers null, n = max) or
+// batched [B, max, feat] with per-problem device counts.
+struct PackSrc {
+    const float* twists; const float* ptf; const int32_t* parent; const int32_t* act;
+    const float* mmul; const float* moff; const int32_t* mact; const int32_t* topo_inv; int J;
+    const int32_t* sli; const float* sloc; const float* srad; int S;
+    const int32_t* cli; const float* cloc; const float* crad; const int32_t* foff; int K;
+    const int32_t* cpairs; const int32_t* cranges; int Q;
+    const float* ws; int ws_max; const int32_t* ws_cnt;
+    const float* wc; int wc_max; const int32_t* wc_cnt;
+    const float* wb; int wb_max; const int32_t* wb_cnt;
+    const float* wh; int wh_max; const int32_t* wh_cnt;
+    const int32_t* sp; int sp_max; const int32_t* sp_cnt;
+    int mode;
+    float margin;
+    int dim;
+};
+
+// Capacity in bytes of one problem's blob (multiple of 256).
+size_t blob_stride(const PackSrc& s);
+cudaError_t launch_pack(const PackSrc& s, int batch, unsigned char* blobs, size_t stride, cudaStream_t st);
+
+struct PlanLaunch {
+    // outputs ([B,...] contiguous, reference layout)
+    float* tree_a; float* tree_b; int32_t* par_a; int32_t* par_b;
+    int32_t* sizes; int32_t* completed; int32_t* iter_count; int32_t* connection; int32_t* solved;
+    float* ktime;
+    // inputs
+    const float* starts; const float* goals; int num_goals; const int32_t* goal_counts;
+    const float* lo; const float* hi;
+    const int32_t* pairs; size_t pairs_stride;   // explicit self pairs (elements of int2 per problem)
+    const int32_t* order;
+    // workspace
+    unsigned char* blobs; size_t blob_stride; int blob_cap;
+    float* radii;                      // [B][2][N]
+    unsigned long long* tstamp;        // [B][2]
+    int32_t* queue;                    // [2]: head, error
+    // shape
+    int B, E, N, dim, J, S, K, Q;
+    // attributes
+    int max_iter, balance_mode, dd, granularity;
+    float step, tree_ratio, dd_alpha, dd_radius, dd_min_radius, edge_res;
+    // tuning
+    int threads, cw, resident;
+    int persistent;
+};
+
+size_t plan_workspace_bytes(int B, int N, size_t blob_stride);
+void plan_carve_workspace(PlanLaunch& L, void* ws, size_t blob_stride);
+cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st);
+cudaError_t launch_extract_paths(int B, int dim, int N, const float* ta, const float* tb, const int32_t* pa,
+                                 const int32_t* pb, const int32_t* conn, const int32_t* solved, int max_len,
+                                 float* paths, int32_t* lengths, float* costs, cudaStream_t st);
+
+// primitives.cu
+cudaError_t launch_nearest(const float* tree, int dim, int N, const int32_t* tree_size, const float* q, int batch,
+                           int32_t* idx, float* dist, unsigned long long* keys, cudaStream_t st);
+cudaError_t launch_extend(const float* tree, int dim, int N, const int32_t* nearest, const float* samples,
+                          int batch, const float* step, float* out, int32_t* parents, int32_t* valid,
+                          cudaStream_t st);
+cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t* pairs, int J, int S, int K,
+                         int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
+                         cudaStream_t st);
+struct FkTables {
+    const float* twists; const float* ptf; const int32_t* parent; const int32_t* act;
+    const float* mmul; const float* moff; const int32_t* mact; const int32_t* topo_inv; int J;
+};
+cudaError_t launch_fk(const FkTables& t, int dim, const float* configs, int n, float* frames, cudaStream_t st);
+cudaError_t launch_halton(int explorer, int n, int dim, const float* lo, const float* hi, float* out,
+                          cudaStream_t st);
+
+// smooth.cu
+cudaError_t launch_smooth(const unsigned char* blob, const int32_t* pairs, int J, int S, int dim,
+                          const float* wp, int P, int W, float margin, float beta, float w_len, float* cost,
+                          float* grad, float* scratch, cudaStream_t st);
+size_t smooth_scratch_bytes(int J, int S, int P, int W);
+
+int device_sm_count();
+size_t device_max_smem();
+
+}  // namespace prrtc

@@ -1,0 +1,289 @@
+// primitives.cu -- standalone kernels: batched nearest neighbour, extend, the
+// batched FK + collision checker, FK and Halton sampling.  sm_100a.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <limits.h>
+#include <math.h>
+
+#include <algorithm>
+
+#include "kernels.h"
+#include "prrtc_device.cuh"
+
+namespace prrtc {
+
+// ============================================================================ nearest neighbour
+
+// Grid (splits, batch): CTA (s, b) scans its slice of the tree for query b and
+// folds its (dsq, index) minimum into keys[b] with a 64-bit atomicMin on
+// (float bits << 32 | index) -- for non-negative floats the bit pattern orders
+// like the value, so the minimum key is the lexicographic (dsq, lowest index)
+// minimum.  NaN slots never win.
+__global__ void __launch_bounds__(256) nn_kernel(const float* __restrict__ tree, int dim, int N,
+                                                 const int32_t* tree_size, const float* __restrict__ q, int batch,
+                                                 int slice, unsigned long long* keys) {
+    const int b = blockIdx.y, tid = threadIdx.x, T = blockDim.x;
+    int n = tree_size ? tree_size[0] : N;
+    n = max(1, min(n, N));
+    const int lo = blockIdx.x * slice;
+    const int hi = min(n, lo + slice);
+    float qr[kDimMax];
+#pragma unroll
+    for (int d = 0; d < kDimMax; ++d) qr[d] = d < dim ? q[(size_t)b * dim + d] : 0.0f;
+    float best = INFINITY;
+    int bi = INT_MAX;
+    if ((N & 3) == 0 && (lo & 3) == 0 && (reinterpret_cast<uintptr_t>(tree) & 15) == 0) {
+        const float4* t4 = reinterpret_cast<const float4*>(tree);
+        const size_t row4 = (size_t)(N >> 2);
+        const int g0 = lo >> 2, g1 = (hi + 3) >> 2;
+        for (int g = g0 + tid; g < g1; g += T) {
+            float4 v = __ldg(t4 + g);
+            float dx = __fsub_rn(v.x, qr[0]), dy = __fsub_rn(v.y, qr[0]), dz = __fsub_rn(v.z, qr[0]),
+                  dw = __fsub_rn(v.w, qr[0]);
+            float ax = __fmul_rn(dx, dx), ay = __fmul_rn(dy, dy), az = __fmul_rn(dz, dz), aw = __fmul_rn(dw, dw);
+#pragma unroll
+            for (int d = 1; d < kDimMax; ++d) {
+                if (d < dim) {
+                    v = __ldg(t4 + d * row4 + g);
+                    dx = __fsub_rn(v.x, qr[d]); dy = __fsub_rn(v.y, qr[d]);
+                    dz = __fsub_rn(v.z, qr[d]); dw = __fsub_rn(v.w, qr[d]);
+                    ax = __fmaf_rn(dx, dx, ax); ay = __fmaf_rn(dy, dy, ay);
+                    az = __fmaf_rn(dz, dz, az); aw = __fmaf_rn(dw, dw, aw);
+                }
+            }
+            const int i0 = g << 2;
+            if (ax < best && i0 < hi) { best = ax; bi = i0; }
+            if (ay < best && i0 + 1 < hi) { best = ay; bi = i0 + 1; }
+            if (az < best && i0 + 2 < hi) { best = az; bi = i0 + 2; }
+            if (aw < best && i0 + 3 < hi) { best = aw; bi = i0 + 3; }
+        }
+    } else {
+        for (int i = lo + tid; i < hi; i += T) {
+            float dd = __fsub_rn(__ldg(tree + i), qr[0]);
+            float acc = __fmul_rn(dd, dd);
+            for (int d = 1; d < dim; ++d) {
+                dd = __fsub_rn(__ldg(tree + (size_t)d * N + i), qr[d]);
+                acc = __fmaf_rn(dd, dd, acc);
+            }
+            if (acc < best) { best = acc; bi = i; }
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float od = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (od < best || (od == best && oi < bi)) { best = od; bi = oi; }
+    }
+    if ((tid & 31) == 0 && bi != INT_MAX) {
+        const unsigned long long key =
+            ((unsigned long long)__float_as_uint(best) << 32) | (unsigned long long)(unsigned)bi;
+        atomicMin(&keys[b], key);
+    }
+}
+
+__global__ void nn_decode_kernel(const unsigned long long* keys, int batch, int32_t* idx, float* dist) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    const unsigned long long k = keys[b];
+    if (k == ~0ull) {
+        idx[b] = 0;
+        dist[b] = INFINITY;
+        return;
+    }
+    idx[b] = (int32_t)(k & 0xffffffffull);
+    dist[b] = __fsqrt_rn(__uint_as_float((unsigned)(k >> 32)));
+}
+
+cudaError_t launch_nearest(const float* tree, int dim, int N, const int32_t* tree_size, const float* q, int batch,
+                           int32_t* idx, float* dist, unsigned long long* keys, cudaStream_t st) {
+    if (batch <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(keys, 0xFF, (size_t)batch * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    // enough CTAs to cover every SM several times; slices are multiples of 1024 nodes
+    const int sms = device_sm_count();
+    int splits = std::max(1, (4 * sms + batch - 1) / batch);
+    int slice = (N + splits - 1) / splits;
+    slice = std::max(1024, (slice + 1023) & ~1023);
+    splits = (N + slice - 1) / slice;
+    nn_kernel<<<dim3(splits, batch), 256, 0, st>>>(tree, dim, N, tree_size, q, batch, slice, keys);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    nn_decode_kernel<<<(batch + 255) / 256, 256, 0, st>>>(keys, batch, idx, dist);
+    return cudaGetLastError();
+}
+
+// ============================================================================ extend
+
+// prrtc_extend.cu:14-73: new = near + (sample - near) * min(1, step / |sample - near|).
+__global__ void extend_kernel(const float* tree, int dim, int N, const int32_t* nearest, const float* samples,
+                              int batch, const float* step, float* out, int32_t* parents, int32_t* valid) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    const int ni = nearest[b];
+    const float s = step[0];
+    float dsq = 0.0f;
+    float nv[kDimMax], sv[kDimMax];
+    for (int d = 0; d < dim; ++d) {
+        nv[d] = tree[(size_t)d * N + ni];
+        sv[d] = samples[(size_t)b * dim + d];
+        const float df = __fsub_rn(sv[d], nv[d]);
+        dsq = d == 0 ? __fmul_rn(df, df) : __fmaf_rn(df, df, dsq);
+    }
+    const float scale = fminf(1.0f, __fdiv_rn(s, __fsqrt_rn(dsq)));
+    for (int d = 0; d < dim; ++d) out[(size_t)b * dim + d] = __fmaf_rn(__fsub_rn(sv[d], nv[d]), scale, nv[d]);
+    parents[b] = ni;
+    valid[b] = 1;
+}
+
+cudaError_t launch_extend(const float* tree, int dim, int N, const int32_t* nearest, const float* samples,
+                          int batch, const float* step, float* out, int32_t* parents, int32_t* valid,
+                          cudaStream_t st) {
+    if (batch <= 0) return cudaSuccess;
+    extend_kernel<<<(batch + 127) / 128, 128, 0, st>>>(tree, dim, N, nearest, samples, batch, step, out, parents,
+                                                       valid);
+    return cudaGetLastError();
+}
+
+// ============================================================================ batched collision check
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Persistent over chunks of CW configurations; the scene is bulk-copied into
+// shared memory once per CTA (bounded wait; on timeout the CTA reads the scene
+// from global memory instead).
+template <int CW>
+__global__ void __launch_bounds__(128) check_kernel(const unsigned char* __restrict__ gblob, int blob_cap,
+                                                    const int32_t* pairs, int J, int S, int K, int Q, int dim,
+                                                    const float* __restrict__ configs, int n, int full_sweep,
+                                                    int32_t* verdicts) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ __align__(8) uint64_t mbar;
+    const int tid = threadIdx.x;
+    const bool staged = blob_cap > 0;
+    const CcBufs B = cc_bufs(dsm + (staged ? blob_cap : 0), J, S, K, Q, CW);
+    Scene sc;
+    if (staged) {
+        const int bytes = min(reinterpret_cast<const BlobHeader*>(gblob)->used_bytes, blob_cap);
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint64_t state;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                         : "=l"(state)
+                         : "r"(smem_u32(&mbar)), "r"(bytes)
+                         : "memory");
+            (void)state;
+            for (int off = 0; off < bytes; off += 16384) {
+                const int m = min(16384, bytes - off);
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        smem_u32(dsm + off)),
+                    "l"(gblob + off), "r"(m), "r"(smem_u32(&mbar))
+                    : "memory");
+            }
+        }
+        uint32_t done = 0;
+        for (int i = 0; i < (1 << 22) && !done; ++i) {
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+                : "=r"(done)
+                : "r"(smem_u32(&mbar))
+                : "memory");
+        }
+        const int all = __syncthreads_and(done ? 1 : 0);
+        sc = scene_view(all ? dsm : gblob);
+    } else {
+        sc = scene_view(gblob);
+    }
+    sc.pairs = reinterpret_cast<const int2*>(pairs);
+    for (int c0 = blockIdx.x * CW; c0 < n; c0 += gridDim.x * CW) {
+        const int nw = min(CW, n - c0);
+        for (int i = tid; i < nw * dim; i += blockDim.x) {
+            const int w = i / dim, d = i - w * dim;
+            B.q[w * kDimMax + d] = configs[(size_t)(c0 + w) * dim + d];
+        }
+        __syncthreads();
+        const uint32_t hit = cc_chunk(sc, B, nw, false, full_sweep != 0);
+        for (int w = tid; w < nw; w += blockDim.x) verdicts[c0 + w] = (hit >> w) & 1u;
+    }
+}
+
+cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t* pairs, int J, int S, int K,
+                         int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
+                         cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    constexpr int CW = 32;
+    const size_t cc = (size_t)cc_smem_bytes(J, S, K, Q, CW);
+    size_t dyn = cc + (size_t)blob_cap;
+    if (dyn + 64 > device_max_smem()) {
+        blob_cap = 0;
+        dyn = cc;
+    }
+    cudaError_t e = cudaFuncSetAttribute(check_kernel<CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, check_kernel<CW>, 128, dyn)) != cudaSuccess)
+        return e;
+    const long long chunks = (n + CW - 1) / CW;
+    const long long grid = std::min<long long>(chunks, (long long)std::max(per_sm, 1) * device_sm_count());
+    check_kernel<CW><<<(unsigned)grid, 128, dyn, st>>>(blob, blob_cap, pairs, J, S, K, Q, dim, configs, n,
+                                                        full_sweep, verdicts);
+    return cudaGetLastError();
+}
+
+// ============================================================================ FK
+
+// One configuration per thread; link frames in thread-local memory (J <= 64),
+// written in output frame order (frame k = sorted joint topo_inv[k]).
+__global__ void fk_kernel(FkTables t, int dim, const float* configs, int n, float* frames) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int J = t.J;
+    float q[kDimMax];
+    for (int d = 0; d < dim; ++d) q[d] = configs[(size_t)c * dim + d];
+    float W[kMaxJoints * 12];
+    for (int j = 0; j < J; ++j) {
+        const JointRec jr = make_joint_rec(j, t.ptf, t.twists, t.parent, t.act, t.mmul, t.moff, t.mact, dim);
+        joint_local(jr, joint_value(jr, q), &W[j * 12]);
+        const int p = jr.idx.x;
+        if (p >= 0 && p < j) compose(&W[p * 12], &W[j * 12], &W[j * 12]);
+    }
+    for (int k = 0; k < J; ++k) {
+        int s = t.topo_inv ? t.topo_inv[k] : k;
+        if (s < 0 || s >= J) s = k;
+        for (int i = 0; i < 12; ++i) frames[((size_t)c * J + k) * 12 + i] = W[s * 12 + i];
+    }
+}
+
+cudaError_t launch_fk(const FkTables& t, int dim, const float* configs, int n, float* frames, cudaStream_t st) {
+    if (n <= 0 || t.J <= 0) return cudaSuccess;
+    fk_kernel<<<(n + 127) / 128, 128, 0, st>>>(t, dim, configs, n, frames);
+    return cudaGetLastError();
+}
+
+// ============================================================================ Halton
+
+__global__ void halton_kernel(int explorer, int n, int dim, const float* lo, const float* hi, float* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int order[16], st[kDimMax];
+    prime_order(explorer, order);
+    for (int d = 0; d < kDimMax; ++d) st[d] = 1;
+    float row[kDimMax];
+    for (int i = 0; i < n; ++i) {
+        halton_sample(order, st, dim, lo, hi, row);
+        for (int d = 0; d < dim; ++d) out[(size_t)i * dim + d] = row[d];
+    }
+}
+
+cudaError_t launch_halton(int explorer, int n, int dim, const float* lo, const float* hi, float* out,
+                          cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    halton_kernel<<<1, 32, 0, st>>>(explorer, n, dim, lo, hi, out);
+    return cudaGetLastError();
+}
+
+}  // namespace prrtc

@@ -1,0 +1,610 @@
+// prrtc_device.cuh -- device building blocks of the B200 pRRTC planner (sm_100a).
+//
+// Layout of one packed scene ("blob"): a 128-byte header followed by 16-byte
+// aligned sections (joints, fine spheres, coarse groups, sphere chunks, world
+// primitives pre-conditioned for the tests, self-collision work items, coarse
+// self pairs).  A planner CTA copies its blob into shared memory with one bulk
+// TMA copy, so every table lookup of the collision check is a shared-memory
+// read (broadcast for world primitives).
+//
+// Collision semantics follow the reference checkers (cuda-rrtc/CUDA/
+// prrtc_planner.cu:234-655): a configuration is in collision when any robot
+// sphere is within `inflate` of a world primitive or another sphere of an active
+// self pair.  inflate = 0 is the binary checker (d <= 0, 252-303); inflate =
+// margin is the differentiable checker, whose verdict "sum of margin penalties
+// < 0" (386) holds exactly when some distance is below the margin.  Coarse
+// gating (426-499, 540-655) only skips work whose verdict is known to be "free".
+#pragma once
+
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+namespace prrtc {
+
+constexpr int kDimMax = 16;
+constexpr int kMaxJoints = 64;
+constexpr int kMaxLinks = 64;
+constexpr int kObsChunk = 32;    // world primitives per work item
+constexpr int kSphChunk = 8;     // fine spheres held in registers per work item
+constexpr int kPairChunk = 32;   // explicit self pairs per work item
+constexpr float kFar = 1.0e18f;  // centre of a sphere that can never collide
+
+// ----------------------------------------------------------------------------- blob
+
+struct BlobHeader {
+    int32_t J, dim, S, S_pad;
+    int32_t K, Q, Ns, Nc;
+    int32_t Nb, Nh, n_sch, n_items;
+    int32_t n_och, gated, enabled, inflate_bits;
+    int32_t o_joint, o_sph, o_sfr, o_grp;
+    int32_t o_sch, o_ws, o_wc, o_wb;
+    int32_t o_wh, o_item, o_cpair, used_bytes;
+    int32_t P, cap_bytes, error, pad0;
+};
+static_assert(sizeof(BlobHeader) == 128, "header must stay 128 bytes");
+
+struct JointRec {     // 96 bytes
+    float4 r0, r1, r2;  // parent transform rows: (R0x R0y R0z tx) ...
+    float4 tv;          // twist linear part, .w = mimic_mul
+    float4 tw;          // twist angular part, .w = mimic_off
+    int4 idx;           // parent, act_idx, mimic_act_idx, kind (0 screw, 1 revolute, 2 prismatic, 3 fixed)
+};
+
+__host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
+__host__ __device__ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
+__host__ __device__ inline int odd_pad(int s) { return s | 1; }
+
+// Capacity of a blob for the given (maximum) counts.  Layout offsets are
+// computed by the pack kernel with the same arithmetic.
+struct BlobLayout {
+    int o_joint, o_sph, o_sfr, o_grp, o_sch, o_ws, o_wc, o_wb, o_wh, o_item, o_cpair, bytes;
+    int sch_cap, item_cap;
+};
+
+__host__ __device__ inline BlobLayout blob_layout(int J, int S, int K, int Q, int P, int Ns, int Nc,
+                                                  int Nb, int Nh) {
+    BlobLayout L;
+    int off = (int)sizeof(BlobHeader);
+    L.sch_cap = cdiv(S, kSphChunk) + K + 1;
+    L.item_cap = cdiv(P, kSphChunk) + 2 * Q + cdiv(P, kPairChunk) + 2;
+    L.o_joint = off; off += J * (int)sizeof(JointRec);
+    L.o_sph = off;   off += S * 16;
+    L.o_sfr = off;   off += align16(S * 4);
+    L.o_grp = off;   off += K * 32;
+    L.o_sch = off;   off += L.sch_cap * 16;
+    L.o_ws = off;    off += Ns * 16;
+    L.o_wc = off;    off += Nc * 32;
+    L.o_wb = off;    off += Nb * 64;
+    L.o_wh = off;    off += Nh * 16;
+    L.o_item = off;  off += L.item_cap * 16;
+    L.o_cpair = off; off += align16(Q * 8);
+    L.bytes = align16(off);
+    return L;
+}
+
+struct Scene {  // typed view of a blob (shared or global memory)
+    const BlobHeader* h;
+    const JointRec* joints;
+    const float4* sph;
+    const int* sfr;
+    const float4* grp;   // [K][2]: (c, r) then int4 bits (frame, s0, s1, 0)
+    const int4* sch;
+    const float4* ws;
+    const float4* wc;    // [Nc][2]
+    const float4* wb;    // [Nb][4]
+    const float4* wh;
+    const int4* item;
+    const int2* cpair;
+    const int2* pairs;   // explicit self-pair list (global memory), for non-block items
+};
+
+__device__ __forceinline__ Scene scene_view(const unsigned char* b) {
+    Scene s;
+    s.h = reinterpret_cast<const BlobHeader*>(b);
+    s.joints = reinterpret_cast<const JointRec*>(b + s.h->o_joint);
+    s.sph = reinterpret_cast<const float4*>(b + s.h->o_sph);
+    s.sfr = reinterpret_cast<const int*>(b + s.h->o_sfr);
+    s.grp = reinterpret_cast<const float4*>(b + s.h->o_grp);
+    s.sch = reinterpret_cast<const int4*>(b + s.h->o_sch);
+    s.ws = reinterpret_cast<const float4*>(b + s.h->o_ws);
+    s.wc = reinterpret_cast<const float4*>(b + s.h->o_wc);
+    s.wb = reinterpret_cast<const float4*>(b + s.h->o_wb);
+    s.wh = reinterpret_cast<const float4*>(b + s.h->o_wh);
+    s.item = reinterpret_cast<const int4*>(b + s.h->o_item);
+    s.cpair = reinterpret_cast<const int2*>(b + s.h->o_cpair);
+    s.pairs = nullptr;
+    return s;
+}
+
+// ----------------------------------------------------------------------------- small helpers
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ int ld_volatile(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+// Dynamic-domain radius updates (prrtc_planner.cu:46-83).  Radii are stored
+// with NaN meaning "unset" (the reference's FLT_MAX), so a byte-fill of 0xFF
+// initialises them.
+__device__ __forceinline__ bool radius_unset(float r) { return !(r < FLT_MAX); }
+
+__device__ inline void radius_shrink(float* radii, int idx, float alpha, float r0, float rmin) {
+    int* ri = reinterpret_cast<int*>(&radii[idx]);
+    int old_i = atomicAdd(ri, 0);
+    for (int guard = 0; guard < (1 << 20); ++guard) {
+        const float old_r = __int_as_float(old_i);
+        const float new_r = radius_unset(old_r) ? r0 : fmaxf(old_r * (1.0f - alpha), rmin);
+        const int prev = atomicCAS(ri, old_i, __float_as_int(new_r));
+        if (prev == old_i) break;
+        old_i = prev;
+    }
+}
+
+__device__ inline void radius_grow(float* radii, int idx, float alpha) {
+    int* ri = reinterpret_cast<int*>(&radii[idx]);
+    int old_i = atomicAdd(ri, 0);
+    for (int guard = 0; guard < (1 << 20); ++guard) {
+        const float old_r = __int_as_float(old_i);
+        if (radius_unset(old_r)) break;
+        const int prev = atomicCAS(ri, old_i, __float_as_int(old_r * (1.0f + alpha)));
+        if (prev == old_i) break;
+        old_i = prev;
+    }
+}
+
+// ----------------------------------------------------------------------------- sampling
+
+// Halton radical inverse (prrtc_planner.cu:144-157): IEEE divide, one FMA per digit.
+__device__ __forceinline__ float halton_next(int base, int& state) {
+    float fraction = 1.0f, result = 0.0f;
+    int n = state;
+    const float fb = (float)base;
+    while (n > 0) {
+        fraction = __fdiv_rn(fraction, fb);
+        result = __fmaf_rn(fraction, (float)(n % base), result);
+        n /= base;
+    }
+    state = state + 1;
+    return result;
+}
+
+// Per-explorer prime order (prrtc_planner.cu:747-758).
+__device__ inline void prime_order(int explorer, int* out16) {
+    int p[16] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59};
+    if (explorer != 0) {
+        unsigned int rng = (unsigned int)explorer * 1664525u + 1013904223u;
+        for (int i = 15; i > 0; --i) {
+            rng = rng * 1664525u + 1013904223u;
+            const int j = (int)(rng % (unsigned int)(i + 1));
+            const int t = p[i];
+            p[i] = p[j];
+            p[j] = t;
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 16; ++d) out16[d] = p[d];
+}
+
+// Sample (784-788): min + val * (max - min) as one FMA.
+__device__ __forceinline__ void halton_sample(const int* order, int* states, int dim, const float* lo,
+                                              const float* hi, float* out) {
+    for (int d = 0; d < dim; ++d) {
+        const float val = halton_next(order[d & 15], states[d]);
+        out[d] = __fmaf_rn(val, __fsub_rn(hi[d], lo[d]), lo[d]);
+    }
+}
+
+// Waypoint count: `granularity`, raised to ceil(|delta|/res) when res > 0.
+__device__ __forceinline__ int edge_waypoints(const float* delta, int dim, int G, float res) {
+    if (!(res > 0.0f)) return G;
+    float s = __fmul_rn(delta[0], delta[0]);
+    for (int d = 1; d < dim; ++d) s = __fmaf_rn(delta[d], delta[d], s);
+    const int n = (int)ceilf(__fdiv_rn(__fsqrt_rn(s), res));
+    return n > G ? n : G;
+}
+
+// ----------------------------------------------------------------------------- FK
+
+// out = a o b ([R|t] as 12 floats, R row-major)
+__device__ __forceinline__ void compose(const float* a, const float* b, float* out) {
+    float o[12];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[i * 3 + j] = fmaf(a[i * 3 + 0], b[j], fmaf(a[i * 3 + 1], b[3 + j], a[i * 3 + 2] * b[6 + j]));
+        o[9 + i] = fmaf(a[i * 3 + 0], b[9], fmaf(a[i * 3 + 1], b[10], fmaf(a[i * 3 + 2], b[11], a[9 + i])));
+    }
+#pragma unroll
+    for (int i = 0; i < 12; ++i) out[i] = o[i];
+}
+
+__device__ __forceinline__ float joint_value(const JointRec& jr, const float* q) {
+    if (jr.idx.z >= 0) return fmaf(jr.tv.w, q[jr.idx.z], jr.tw.w);
+    if (jr.idx.y >= 0) return q[jr.idx.y];
+    return 0.0f;
+}
+
+// Local transform parent_tf o exp(twist * v) of one joint, written as 12 floats.
+__device__ inline void joint_local(const JointRec& jr, float v, float* out) {
+    const float P[12] = {jr.r0.x, jr.r0.y, jr.r0.z, jr.r1.x, jr.r1.y, jr.r1.z,
+                         jr.r2.x, jr.r2.y, jr.r2.z, jr.r0.w, jr.r1.w, jr.r2.w};
+    const int kind = jr.idx.w;
+    if (kind == 3) {
+#pragma unroll
+        for (int i = 0; i < 12; ++i) out[i] = P[i];
+        return;
+    }
+    float E[12];
+    if (kind == 2) {  // pure translation along v
+        E[0] = 1; E[1] = 0; E[2] = 0; E[3] = 0; E[4] = 1; E[5] = 0; E[6] = 0; E[7] = 0; E[8] = 1;
+        E[9] = jr.tv.x * v; E[10] = jr.tv.y * v; E[11] = jr.tv.z * v;
+    } else {
+        const float wx = jr.tw.x * v, wy = jr.tw.y * v, wz = jr.tw.z * v;
+        const float th2 = fmaf(wx, wx, fmaf(wy, wy, wz * wz));
+        const float th = sqrtf(th2);
+        float A, B, Cc;
+        if (kind == 1) {  // unit axis: th = |v|, R = I + sin(v) K + (1-cos(v)) K^2 with K from the axis
+            float s, c;
+            sincosf(v, &s, &c);
+            const float ax = jr.tw.x, ay = jr.tw.y, az = jr.tw.z;
+            const float oc = 1.0f - c;
+            E[0] = fmaf(oc, ax * ax - 1.0f, 1.0f); E[1] = fmaf(oc, ax * ay, -s * az); E[2] = fmaf(oc, ax * az, s * ay);
+            E[3] = fmaf(oc, ay * ax, s * az); E[4] = fmaf(oc, ay * ay - 1.0f, 1.0f); E[5] = fmaf(oc, ay * az, -s * ax);
+            E[6] = fmaf(oc, az * ax, -s * ay); E[7] = fmaf(oc, az * ay, s * ax); E[8] = fmaf(oc, az * az - 1.0f, 1.0f);
+            E[9] = 0; E[10] = 0; E[11] = 0;
+        } else {
+            if (th < 1e-4f) {
+                A = 1.0f - th2 * (1.0f / 6.0f);
+                B = 0.5f - th2 * (1.0f / 24.0f);
+                Cc = (1.0f / 6.0f) - th2 * (1.0f / 120.0f);
+            } else {
+                float s, c;
+                sincosf(th, &s, &c);
+                A = s / th;
+                B = (1.0f - c) / th2;
+                Cc = (th - s) / (th2 * th);
+            }
+            const float K[9] = {0, -wz, wy, wz, 0, -wx, -wy, wx, 0};
+            const float K2[9] = {wx * wx - th2, wx * wy, wx * wz, wy * wx, wy * wy - th2, wy * wz,
+                                 wz * wx, wz * wy, wz * wz - th2};
+            float V[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                E[i] = fmaf(A, K[i], B * K2[i]);
+                V[i] = fmaf(B, K[i], Cc * K2[i]);
+            }
+            E[0] += 1.0f; E[4] += 1.0f; E[8] += 1.0f;
+            V[0] += 1.0f; V[4] += 1.0f; V[8] += 1.0f;
+            const float vx = jr.tv.x * v, vy = jr.tv.y * v, vz = jr.tv.z * v;
+            E[9] = fmaf(V[0], vx, fmaf(V[1], vy, V[2] * vz));
+            E[10] = fmaf(V[3], vx, fmaf(V[4], vy, V[5] * vz));
+            E[11] = fmaf(V[6], vx, fmaf(V[7], vy, V[8] * vz));
+        }
+    }
+    compose(P, E, out);
+}
+
+// Joint record from the reference tables: parent_tf quaternion (normalised) as a
+// rotation matrix, twist split into linear/angular parts, joint kind.
+__device__ inline JointRec make_joint_rec(int j, const float* ptf, const float* twists, const int32_t* parent,
+                                          const int32_t* act, const float* mmul, const float* moff,
+                                          const int32_t* mact, int dim) {
+    const float* q = &ptf[j * 7];
+    float w = q[0], x = q[1], y = q[2], z = q[3];
+    const float n = sqrtf(w * w + x * x + y * y + z * z);
+    if (n > 0.0f) { w /= n; x /= n; y /= n; z /= n; } else { w = 1.0f; x = y = z = 0.0f; }
+    JointRec r;
+    r.r0 = make_float4(1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y), q[4]);
+    r.r1 = make_float4(2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x), q[5]);
+    r.r2 = make_float4(2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y), q[6]);
+    const float* tw = &twists[j * 6];
+    r.tv = make_float4(tw[0], tw[1], tw[2], mmul ? mmul[j] : 1.0f);
+    r.tw = make_float4(tw[3], tw[4], tw[5], moff ? moff[j] : 0.0f);
+    const float vn = sqrtf(tw[0] * tw[0] + tw[1] * tw[1] + tw[2] * tw[2]);
+    const float wn = sqrtf(tw[3] * tw[3] + tw[4] * tw[4] + tw[5] * tw[5]);
+    int kind = 0;
+    if (vn < 1e-12f && wn < 1e-12f) kind = 3;
+    else if (wn < 1e-12f) kind = 2;
+    else if (vn < 1e-12f && fabsf(wn - 1.0f) < 1e-6f) kind = 1;
+    int a = act ? act[j] : -1;
+    int ma = mact ? mact[j] : -1;
+    if (a >= dim) a = -1;
+    if (ma >= dim) ma = -1;
+    int par = parent ? parent[j] : -1;
+    if (par >= j) par = -1;
+    r.idx = make_int4(par, a, ma, kind);
+    return r;
+}
+
+// ----------------------------------------------------------------------------- primitive tests
+
+__device__ __forceinline__ float4 xform_point(const float* F, float4 l) {
+    float4 r;
+    r.x = fmaf(F[0], l.x, fmaf(F[1], l.y, fmaf(F[2], l.z, F[9])));
+    r.y = fmaf(F[3], l.x, fmaf(F[4], l.y, fmaf(F[5], l.z, F[10])));
+    r.z = fmaf(F[6], l.x, fmaf(F[7], l.y, fmaf(F[8], l.z, F[11])));
+    r.w = l.w;
+    return r;
+}
+
+// c.w carries the robot sphere radius plus the inflation margin.
+__device__ __forceinline__ bool hit_sphere(float4 c, float4 o) {
+    const float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float t = c.w + o.w;
+    return d2 <= t * t;
+}
+
+__device__ __forceinline__ bool hit_capsule(float4 c, float4 p1r, float4 dl) {
+    const float wx = c.x - p1r.x, wy = c.y - p1r.y, wz = c.z - p1r.z;
+    float t = fmaf(wx, dl.x, fmaf(wy, dl.y, wz * dl.z)) * dl.w;
+    t = fminf(fmaxf(t, 0.0f), 1.0f);
+    const float ex = fmaf(-t, dl.x, wx), ey = fmaf(-t, dl.y, wy), ez = fmaf(-t, dl.z, wz);
+    const float d2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+    const float th = c.w + p1r.w;
+    return d2 <= th * th;
+}
+
+__device__ __forceinline__ bool hit_box(float4 c, float4 b0, float4 a1, float4 a2, float4 a3) {
+    const float px = c.x - b0.x, py = c.y - b0.y, pz = c.z - b0.z;
+    const float q1 = fmaxf(fabsf(fmaf(px, a1.x, fmaf(py, a1.y, pz * a1.z))) - a1.w, 0.0f);
+    const float q2 = fmaxf(fabsf(fmaf(px, a2.x, fmaf(py, a2.y, pz * a2.z))) - a2.w, 0.0f);
+    const float q3 = fmaxf(fabsf(fmaf(px, a3.x, fmaf(py, a3.y, pz * a3.z))) - a3.w, 0.0f);
+    const float d2 = fmaf(q1, q1, fmaf(q2, q2, q3 * q3));
+    return d2 <= c.w * c.w;
+}
+
+__device__ __forceinline__ bool hit_halfspace(float4 c, float4 h) {
+    return fmaf(h.x, c.x, fmaf(h.y, c.y, h.z * c.z)) - h.w <= c.w;
+}
+
+// One obstacle chunk of one type against up to 8 sphere centres held in registers.
+// Returns true on the first hit unless full_sweep.
+__device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int och, const float4 (&s)[kSphChunk],
+                                                     bool full_sweep) {
+    const BlobHeader& h = *sc.h;
+    int c = och;
+    bool hit = false;
+    const int ns = cdiv(h.Ns, kObsChunk), nc = cdiv(h.Nc, kObsChunk), nb = cdiv(h.Nb, kObsChunk);
+    if (c < ns) {
+        const int o0 = c * kObsChunk, o1 = min(h.Ns, o0 + kObsChunk);
+        for (int o = o0; o < o1; ++o) {
+            const float4 ob = sc.ws[o];
+#pragma unroll
+            for (int k = 0; k < kSphChunk; ++k) hit |= hit_sphere(s[k], ob);
+            if (hit && !full_sweep) return true;
+        }
+        return hit;
+    }
+    c -= ns;
+    if (c < nc) {
+        const int o0 = c * kObsChunk, o1 = min(h.Nc, o0 + kObsChunk);
+        for (int o = o0; o < o1; ++o) {
+            const float4 p = sc.wc[2 * o], d = sc.wc[2 * o + 1];
+#pragma unroll
+            for (int k = 0; k < kSphChunk; ++k) hit |= hit_capsule(s[k], p, d);
+            if (hit && !full_sweep) return true;
+        }
+        return hit;
+    }
+    c -= nc;
+    if (c < nb) {
+        const int o0 = c * kObsChunk, o1 = min(h.Nb, o0 + kObsChunk);
+        for (int o = o0; o < o1; ++o) {
+            const float4 b0 = sc.wb[4 * o], a1 = sc.wb[4 * o + 1], a2 = sc.wb[4 * o + 2], a3 = sc.wb[4 * o + 3];
+#pragma unroll
+            for (int k = 0; k < kSphChunk; ++k) hit |= hit_box(s[k], b0, a1, a2, a3);
+            if (hit && !full_sweep) return true;
+        }
+        return hit;
+    }
+    c -= nb;
+    {
+        const int o0 = c * kObsChunk, o1 = min(h.Nh, o0 + kObsChunk);
+        for (int o = o0; o < o1; ++o) {
+            const float4 hs = sc.wh[o];
+#pragma unroll
+            for (int k = 0; k < kSphChunk; ++k) hit |= hit_halfspace(s[k], hs);
+            if (hit && !full_sweep) return true;
+        }
+    }
+    return hit;
+}
+
+// ----------------------------------------------------------------------------- CTA-cooperative check
+
+// Shared-memory work buffers of the collision check for a chunk of CW waypoints.
+struct CcBufs {
+    float* q;        // [CW][kDimMax]
+    float* pose;     // [CW][J][12]
+    float4* ctr;     // [CW][S_pad]
+    float4* cctr;    // [CW][K]
+    uint32_t* dirty; // [CW][KW]
+    uint32_t* gate;  // [CW][QW]
+    uint32_t* hit;   // [1]
+};
+
+__host__ __device__ inline int cc_smem_bytes(int J, int S, int K, int Q, int CW) {
+    const int S_pad = odd_pad(S);
+    const int KW = cdiv(K > 0 ? K : 1, 32), QW = cdiv(Q > 0 ? Q : 1, 32);
+    int b = 0;
+    b += align16(CW * kDimMax * 4);
+    b += align16(CW * J * 48);
+    b += CW * S_pad * 16;
+    b += CW * K * 16;
+    b += align16(CW * KW * 4);
+    b += align16(CW * QW * 4);
+    b += 16;
+    return b;
+}
+
+__device__ inline CcBufs cc_bufs(unsigned char* base, int J, int S, int K, int Q, int CW) {
+    const int S_pad = odd_pad(S);
+    const int KW = cdiv(K > 0 ? K : 1, 32), QW = cdiv(Q > 0 ? Q : 1, 32);
+    CcBufs b;
+    unsigned char* p = base;
+    b.q = reinterpret_cast<float*>(p);        p += align16(CW * kDimMax * 4);
+    b.pose = reinterpret_cast<float*>(p);     p += align16(CW * J * 48);
+    b.ctr = reinterpret_cast<float4*>(p);     p += CW * S_pad * 16;
+    b.cctr = reinterpret_cast<float4*>(p);    p += CW * K * 16;
+    b.dirty = reinterpret_cast<uint32_t*>(p); p += align16(CW * KW * 4);
+    b.gate = reinterpret_cast<uint32_t*>(p);  p += align16(CW * QW * 4);
+    b.hit = reinterpret_cast<uint32_t*>(p);
+    return b;
+}
+
+// Collision check of nw (<= CW <= 32) configurations already in B.q.  Every
+// thread of the CTA must call it.  edge_mode: stop all work at the first hit
+// (the whole edge is rejected).  Otherwise each configuration stops at its own
+// first hit, or never with full_sweep.  Returns the hit bit mask (bit w =
+// configuration w in collision).
+__device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bool edge_mode, bool full_sweep) {
+    const BlobHeader& h = *sc.h;
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int J = h.J, S = h.S, S_pad = h.S_pad, K = h.K, Q = h.Q;
+    const bool gated = h.gated != 0;
+    const float inflate = __int_as_float(h.inflate_bits);
+    const int KW = cdiv(K > 0 ? K : 1, 32), QW = cdiv(Q > 0 ? Q : 1, 32);
+    volatile uint32_t* vhit = B.hit;
+
+    if (!h.enabled) {
+        __syncthreads();
+        return 0u;
+    }
+    if (tid == 0) *vhit = 0u;
+    if (gated) {
+        for (int i = tid; i < nw * KW; i += T) B.dirty[i] = 0u;
+        for (int i = tid; i < nw * QW; i += T) B.gate[i] = 0u;
+    }
+    // A: local joint transforms, one (waypoint, joint) per thread
+    for (int it = tid; it < nw * J; it += T) {
+        const int w = it / J, j = it - w * J;
+        const JointRec& jr = sc.joints[j];
+        joint_local(jr, joint_value(jr, &B.q[w * kDimMax]), &B.pose[(w * J + j) * 12]);
+    }
+    __syncthreads();
+    // B: chain composition in topological order, one waypoint per thread
+    for (int w = tid; w < nw; w += T) {
+        float* P = &B.pose[w * J * 12];
+        for (int j = 0; j < J; ++j) {
+            const int p = sc.joints[j].idx.x;
+            if (p >= 0 && p < j) compose(&P[p * 12], &P[j * 12], &P[j * 12]);
+        }
+    }
+    __syncthreads();
+    // C: sphere centres (fine, and coarse when gated)
+    for (int it = tid; it < nw * S; it += T) {
+        const int w = it / S, s = it - w * S;
+        const int f = sc.sfr[s];
+        float4 l = sc.sph[s];
+        l.w += inflate;
+        float4 c;
+        if (f >= 0) c = xform_point(&B.pose[(w * J + f) * 12], l);
+        else c = make_float4(kFar, kFar, kFar, l.w);
+        B.ctr[w * S_pad + s] = c;
+    }
+    if (gated) {
+        for (int it = tid; it < nw * K; it += T) {
+            const int w = it / K, k = it - w * K;
+            float4 l = sc.grp[2 * k];
+            l.w += inflate;
+            const int f = __float_as_int(sc.grp[2 * k + 1].x);
+            float4 c;
+            if (f >= 0) c = xform_point(&B.pose[(w * J + f) * 12], l);
+            else c = make_float4(kFar, kFar, kFar, l.w);
+            B.cctr[w * K + k] = c;
+        }
+    }
+    __syncthreads();
+    // D: coarse pre-pass -> dirty groups and touching coarse self pairs
+    if (gated) {
+        const int n_cw = nw * K * h.n_och;
+        for (int it = tid; it < n_cw + nw * Q; it += T) {
+            if (it < n_cw) {
+                const int och = it / (nw * K), r = it - och * (nw * K);
+                const int k = r / nw, w = r - k * nw;
+                if (B.dirty[w * KW + (k >> 5)] & (1u << (k & 31))) continue;
+                float4 s[kSphChunk];
+                s[0] = B.cctr[w * K + k];
+#pragma unroll
+                for (int m = 1; m < kSphChunk; ++m) s[m] = make_float4(kFar, kFar, kFar, 0.0f);
+                if (obstacles_vs_spheres(sc, och, s, false)) atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
+            } else {
+                const int r = it - n_cw;
+                const int qq = r / nw, w = r - qq * nw;
+                const int2 cp = sc.cpair[qq];
+                if (cp.x < 0 || cp.y < 0 || cp.x >= K || cp.y >= K) continue;
+                const float4 a = B.cctr[w * K + cp.x], b = B.cctr[w * K + cp.y];
+                const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+                const float t = a.w + b.w - inflate;
+                if (fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= t * t) atomicOr(&B.gate[w * QW + (qq >> 5)], 1u << (qq & 31));
+            }
+        }
+        __syncthreads();
+    }
+    // E: fine work items.  World: (obstacle chunk, sphere chunk, waypoint) with the
+    // obstacle chunk slowest so a warp reads the same primitive (broadcast).
+    // Self: (item, waypoint).
+    const int n_world = nw * h.n_sch * h.n_och;
+    const int n_total = n_world + nw * h.n_items;
+    for (int it = tid; it < n_total; it += T) {
+        int w;
+        bool hit = false;
+        if (it < n_world) {
+            const int och = it / (nw * h.n_sch), r = it - och * (nw * h.n_sch);
+            const int si = r / nw;
+            w = r - si * nw;
+            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) continue;
+            const int4 ch = sc.sch[si];
+            if (gated && ch.z >= 0 && !(B.dirty[w * KW + (ch.z >> 5)] & (1u << (ch.z & 31)))) continue;
+            float4 s[kSphChunk];
+#pragma unroll
+            for (int m = 0; m < kSphChunk; ++m)
+                s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : make_float4(kFar, kFar, kFar, 0.0f);
+            hit = obstacles_vs_spheres(sc, och, s, full_sweep);
+        } else {
+            const int r = it - n_world;
+            const int ii = r / nw;
+            w = r - ii * nw;
+            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) continue;
+            const int4 item = sc.item[ii];
+            if (gated && item.w >= 0 && !(B.gate[w * QW + (item.w >> 5)] & (1u << (item.w & 31)))) continue;
+            const float4* C = &B.ctr[w * S_pad];
+            if (item.y >= 0) {  // dense block: spheres [a0, a0+na) x [b0, b0+nb)
+                const int na = item.z >> 16, nb = item.z & 0xffff;
+                float4 a[kSphChunk];
+#pragma unroll
+                for (int m = 0; m < kSphChunk; ++m) {
+                    a[m] = (m < na) ? C[item.x + m] : make_float4(kFar, kFar, kFar, 0.0f);
+                    a[m].w -= inflate;
+                }
+                for (int bb = 0; bb < nb; ++bb) {
+                    const float4 b = C[item.y + bb];
+#pragma unroll
+                    for (int m = 0; m < kSphChunk; ++m) hit |= hit_sphere(a[m], b);
+                    if (hit && !full_sweep) break;
+                }
+            } else {  // explicit pairs [p0, p0+count) of the pair list (global memory)
+                const int p1 = min(item.x + item.z, h.P);
+                for (int p = item.x; p < p1; ++p) {
+                    const int2 pr = __ldg(&sc.pairs[p]);
+                    if (pr.x < 0 || pr.y < 0 || pr.x >= S || pr.y >= S) continue;
+                    const float4 a = C[pr.x], b = C[pr.y];
+                    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+                    const float t = a.w + b.w - inflate;
+                    hit |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= t * t;
+                    if (hit && !full_sweep) break;
+                }
+            }
+        }
+        if (hit) atomicOr(B.hit, 1u << w);
+    }
+    __syncthreads();
+    return *vhit;
+}
+
+}  // namespace prrtc

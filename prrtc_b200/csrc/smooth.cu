@@ -1,0 +1,273 @@
+// smooth.cu -- hand-written adjoint of the post-plan smoothing cost.  sm_100a.
+//
+// For a path of W waypoints q_w (dim each):
+//   C = sum_w sum_pairs softplus_beta(margin - d_pair(q_w)) + w_len * sum_w |q_{w+1} - q_w|^2
+// over every (robot sphere, world primitive) pair and every self pair, with
+// softplus_beta(x) = log(1 + exp(beta x)) / beta.
+//
+// Backward pass per waypoint, one warp per waypoint, nothing stored between the
+// forward and backward sweeps except per-sphere centres:
+//   1. recompute FK (joint-local transforms in parallel over lanes, chain
+//      composition on lane 0) and the sphere centres c_s;
+//   2. g_s = dC/dc_s from every pair: -sigmoid(beta (m - d)) * dd/dc_s;
+//   3. per frame f: G_f = sum g_s, M_f = sum c_s x g_s over its spheres, then
+//      folded into parents in reverse topological order (subtree sums);
+//   4. joint j with world pose (R_j, t_j) and twist (v, w):
+//        dC/dv_j = (R_j w) . (M_j - t_j x G_j) + (R_j v) . G_j
+//      (a point p below joint j moves with dp/dv_j = (R_j w) x (p - t_j) + R_j v);
+//   5. dC/dq_a = sum over joints driven by a of dv_j/dq_a * dC/dv_j (1 for an
+//      actuated joint, mimic_mul for a mimic joint) plus the length term.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "kernels.h"
+#include "prrtc_device.cuh"
+
+namespace prrtc {
+
+__device__ __forceinline__ float softplus_b(float x, float beta) {
+    const float z = beta * x;
+    return (z > 0.0f ? z + log1pf(expf(-z)) : log1pf(expf(z))) / beta;
+}
+
+__device__ __forceinline__ float sigmoid_f(float z) { return 1.0f / (1.0f + expf(-z)); }
+
+struct SmoothArgs {
+    const unsigned char* blob;
+    const int2* pairs;
+    int J, S, dim;
+    const float* wp;
+    int P, W;
+    float margin, beta, w_len;
+    float* cost;
+    float* grad;
+};
+
+// per-warp shared memory: pose J*12, ctr S*4, g S*4, acc J*8, dv J, q dim (padded)
+__host__ __device__ inline int smooth_warp_floats(int J, int S) {
+    return (J * 12 + S * 4 + S * 4 + J * 8 + J + kDimMax + 3) & ~3;  // keep every warp slice 16-byte aligned
+}
+
+// accumulate the pair term for distance d with gradient direction u (dd/dc = u)
+__device__ __forceinline__ void pair_term(float d, float margin, float beta, float& cost, float& sig) {
+    const float x = margin - d;
+    cost += softplus_b(x, beta);
+    sig = sigmoid_f(beta * x);
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
+    extern __shared__ __align__(16) float smf[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * WARPS + warp;
+    if (c >= a.P * a.W) return;
+    const int p = c / a.W, w = c - p * a.W;
+    const Scene sc = scene_view(a.blob);
+    const BlobHeader& h = *sc.h;
+    const int J = a.J, S = a.S, dim = a.dim;
+    float* base = smf + (size_t)warp * smooth_warp_floats(J, S);
+    float* pose = base;
+    float4* ctr = reinterpret_cast<float4*>(pose + J * 12);
+    float4* g = ctr + S;
+    float* acc = reinterpret_cast<float*>(g + S);  // [J][8]: G xyz, M xyz
+    float* dv = acc + J * 8;
+    float* q = dv + J;
+    const float* qw = a.wp + ((size_t)p * a.W + w) * dim;
+    if (lane < dim) q[lane] = qw[lane];
+    __syncwarp();
+    // 1. FK (recomputed) and centres
+    for (int j = lane; j < J; j += 32) {
+        const JointRec& jr = sc.joints[j];
+        joint_local(jr, joint_value(jr, q), &pose[j * 12]);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        for (int j = 0; j < J; ++j) {
+            const int pj = sc.joints[j].idx.x;
+            if (pj >= 0 && pj < j) compose(&pose[pj * 12], &pose[j * 12], &pose[j * 12]);
+        }
+    }
+    __syncwarp();
+    for (int s = lane; s < S; s += 32) {
+        const int f = sc.sfr[s];
+        const float4 l = sc.sph[s];
+        ctr[s] = f >= 0 ? xform_point(&pose[f * 12], l) : make_float4(kFar, kFar, kFar, l.w);
+        g[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    for (int i = lane; i < J * 8; i += 32) acc[i] = 0.0f;
+    __syncwarp();
+    // 2a. world pairs: one sphere per lane
+    float cost = 0.0f;
+    for (int s = lane; s < S; s += 32) {
+        if (sc.sfr[s] < 0) continue;
+        const float4 cs = ctr[s];
+        const float r = cs.w;
+        float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        for (int o = 0; o < h.Ns; ++o) {
+            const float4 ob = sc.ws[o];
+            const float dx = cs.x - ob.x, dy = cs.y - ob.y, dz = cs.z - ob.z;
+            const float n = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+            float sig;
+            pair_term(n - r - ob.w, a.margin, a.beta, cost, sig);
+            const float k = n > 0.0f ? -sig / n : 0.0f;
+            gx = fmaf(k, dx, gx); gy = fmaf(k, dy, gy); gz = fmaf(k, dz, gz);
+        }
+        for (int o = 0; o < h.Nc; ++o) {
+            const float4 p1 = sc.wc[2 * o], dl = sc.wc[2 * o + 1];
+            const float wx = cs.x - p1.x, wy = cs.y - p1.y, wz = cs.z - p1.z;
+            float t = fmaf(wx, dl.x, fmaf(wy, dl.y, wz * dl.z)) * dl.w;
+            t = fminf(fmaxf(t, 0.0f), 1.0f);
+            const float ex = fmaf(-t, dl.x, wx), ey = fmaf(-t, dl.y, wy), ez = fmaf(-t, dl.z, wz);
+            const float n = sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
+            float sig;
+            pair_term(n - r - p1.w, a.margin, a.beta, cost, sig);
+            const float k = n > 0.0f ? -sig / n : 0.0f;
+            gx = fmaf(k, ex, gx); gy = fmaf(k, ey, gy); gz = fmaf(k, ez, gz);
+        }
+        for (int o = 0; o < h.Nb; ++o) {
+            const float4 b0 = sc.wb[4 * o], ax[3] = {sc.wb[4 * o + 1], sc.wb[4 * o + 2], sc.wb[4 * o + 3]};
+            const float px = cs.x - b0.x, py = cs.y - b0.y, pz = cs.z - b0.z;
+            float l[3], qv[3], out2 = 0.0f, qmax = -INFINITY;
+            int kmax = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                l[k] = fmaf(px, ax[k].x, fmaf(py, ax[k].y, pz * ax[k].z));
+                qv[k] = fabsf(l[k]) - ax[k].w;
+                if (qv[k] > 0.0f) out2 = fmaf(qv[k], qv[k], out2);
+                if (qv[k] > qmax) { qmax = qv[k]; kmax = k; }
+            }
+            float d, ddx = 0.0f, ddy = 0.0f, ddz = 0.0f;
+            if (out2 > 0.0f) {
+                const float n = sqrtf(out2);
+                d = n - r;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (qv[k] > 0.0f) {
+                        const float coef = copysignf(qv[k] / n, l[k]);
+                        ddx = fmaf(coef, ax[k].x, ddx); ddy = fmaf(coef, ax[k].y, ddy); ddz = fmaf(coef, ax[k].z, ddz);
+                    }
+                }
+            } else {
+                d = qmax - r;
+                const float sgn = copysignf(1.0f, l[kmax]);
+                ddx = sgn * ax[kmax].x; ddy = sgn * ax[kmax].y; ddz = sgn * ax[kmax].z;
+            }
+            float sig;
+            pair_term(d, a.margin, a.beta, cost, sig);
+            gx = fmaf(-sig, ddx, gx); gy = fmaf(-sig, ddy, gy); gz = fmaf(-sig, ddz, gz);
+        }
+        for (int o = 0; o < h.Nh; ++o) {
+            const float4 hs = sc.wh[o];
+            const float d = fmaf(hs.x, cs.x, fmaf(hs.y, cs.y, hs.z * cs.z)) - hs.w - r;
+            float sig;
+            pair_term(d, a.margin, a.beta, cost, sig);
+            gx = fmaf(-sig, hs.x, gx); gy = fmaf(-sig, hs.y, gy); gz = fmaf(-sig, hs.z, gz);
+        }
+        g[s] = make_float4(gx, gy, gz, 0.0f);
+    }
+    __syncwarp();
+    // 2b. self pairs (explicit list): shared-memory atomics into both spheres
+    for (int k = lane; k < h.P; k += 32) {
+        const int2 pr = __ldg(&a.pairs[k]);
+        if (pr.x < 0 || pr.y < 0 || pr.x >= S || pr.y >= S) continue;
+        if (sc.sfr[pr.x] < 0 || sc.sfr[pr.y] < 0) continue;
+        const float4 ci = ctr[pr.x], cj = ctr[pr.y];
+        const float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+        const float n = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        float sig;
+        pair_term(n - ci.w - cj.w, a.margin, a.beta, cost, sig);
+        const float kk = n > 0.0f ? -sig / n : 0.0f;
+        atomicAdd(&g[pr.x].x, kk * dx); atomicAdd(&g[pr.x].y, kk * dy); atomicAdd(&g[pr.x].z, kk * dz);
+        atomicAdd(&g[pr.y].x, -kk * dx); atomicAdd(&g[pr.y].y, -kk * dy); atomicAdd(&g[pr.y].z, -kk * dz);
+    }
+    __syncwarp();
+    // 3. frame sums
+    for (int s = lane; s < S; s += 32) {
+        const int f = sc.sfr[s];
+        if (f < 0) continue;
+        const float4 cs = ctr[s], gs = g[s];
+        float* A = &acc[f * 8];
+        atomicAdd(&A[0], gs.x); atomicAdd(&A[1], gs.y); atomicAdd(&A[2], gs.z);
+        atomicAdd(&A[3], cs.y * gs.z - cs.z * gs.y);
+        atomicAdd(&A[4], cs.z * gs.x - cs.x * gs.z);
+        atomicAdd(&A[5], cs.x * gs.y - cs.y * gs.x);
+    }
+    __syncwarp();
+    // 4. reverse sweep
+    if (lane == 0) {
+        for (int j = J - 1; j >= 0; --j) {
+            const JointRec& jr = sc.joints[j];
+            const float* F = &pose[j * 12];
+            float* A = &acc[j * 8];
+            const float wx = fmaf(F[0], jr.tw.x, fmaf(F[1], jr.tw.y, F[2] * jr.tw.z));
+            const float wy = fmaf(F[3], jr.tw.x, fmaf(F[4], jr.tw.y, F[5] * jr.tw.z));
+            const float wz = fmaf(F[6], jr.tw.x, fmaf(F[7], jr.tw.y, F[8] * jr.tw.z));
+            const float vx = fmaf(F[0], jr.tv.x, fmaf(F[1], jr.tv.y, F[2] * jr.tv.z));
+            const float vy = fmaf(F[3], jr.tv.x, fmaf(F[4], jr.tv.y, F[5] * jr.tv.z));
+            const float vz = fmaf(F[6], jr.tv.x, fmaf(F[7], jr.tv.y, F[8] * jr.tv.z));
+            const float tx = F[9], ty = F[10], tz = F[11];
+            const float mx = A[3] - (ty * A[2] - tz * A[1]);
+            const float my = A[4] - (tz * A[0] - tx * A[2]);
+            const float mz = A[5] - (tx * A[1] - ty * A[0]);
+            dv[j] = wx * mx + wy * my + wz * mz + vx * A[0] + vy * A[1] + vz * A[2];
+            const int pj = jr.idx.x;
+            if (pj >= 0 && pj < j) {
+                float* B = &acc[pj * 8];
+#pragma unroll
+                for (int i = 0; i < 6; ++i) B[i] += A[i];
+            }
+        }
+    }
+    __syncwarp();
+    // 5. joint-space gradient + length term
+    float lenc = 0.0f;
+    if (lane < dim) {
+        float gq = 0.0f;
+        for (int j = 0; j < J; ++j) {
+            const JointRec& jr = sc.joints[j];
+            if (jr.idx.z >= 0) {
+                if (jr.idx.z == lane) gq = fmaf(jr.tv.w, dv[j], gq);
+            } else if (jr.idx.y == lane) {
+                gq += dv[j];
+            }
+        }
+        const float qc = q[lane];
+        if (w + 1 < a.W) {
+            const float dn = a.wp[((size_t)p * a.W + w + 1) * dim + lane] - qc;
+            gq -= 2.0f * a.w_len * dn;
+            lenc = a.w_len * dn * dn;
+        }
+        if (w > 0) {
+            const float dp = qc - a.wp[((size_t)p * a.W + w - 1) * dim + lane];
+            gq += 2.0f * a.w_len * dp;
+        }
+        if (a.grad) a.grad[((size_t)p * a.W + w) * dim + lane] = gq;
+    }
+    cost += lenc;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cost += __shfl_xor_sync(0xffffffffu, cost, off);
+    if (lane == 0) atomicAdd(&a.cost[p], cost);
+}
+
+size_t smooth_scratch_bytes(int, int, int, int) { return 0; }
+
+cudaError_t launch_smooth(const unsigned char* blob, const int32_t* pairs, int J, int S, int dim, const float* wp,
+                          int P, int W, float margin, float beta, float w_len, float* cost, float* grad, float*,
+                          cudaStream_t st) {
+    if (P <= 0 || W <= 0) return cudaSuccess;
+    constexpr int WARPS = 4;
+    cudaError_t e = cudaMemsetAsync(cost, 0, (size_t)P * sizeof(float), st);
+    if (e != cudaSuccess) return e;
+    const size_t smem = (size_t)WARPS * smooth_warp_floats(J, S) * sizeof(float);
+    if (smem > 48 * 1024) {
+        if ((e = cudaFuncSetAttribute(smooth_kernel<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem)) != cudaSuccess)
+            return e;
+    }
+    SmoothArgs a{blob, reinterpret_cast<const int2*>(pairs), J, S, dim, wp, P, W, margin, beta, w_len, cost, grad};
+    const long long n = (long long)P * W;
+    smooth_kernel<WARPS><<<(unsigned)((n + WARPS - 1) / WARPS), WARPS * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace prrtc

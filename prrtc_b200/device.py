@@ -1,0 +1,124 @@
+"""Device-side views of collision contexts and small torch helpers.
+
+torch provides device memory and streams; the computation itself is in
+libprrtc_b200.so.  A ``DeviceContext`` holds the collision_context tensors of
+one robot + world on a CUDA device and fills the C structs of the C-ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+
+ROBOT_SPEC = {
+    "fk_twists": (torch.float32, 6), "fk_parent_tf": (torch.float32, 7),
+    "fk_parent_idx": (torch.int32, 0), "fk_act_idx": (torch.int32, 0),
+    "fk_mimic_mul": (torch.float32, 0), "fk_mimic_off": (torch.float32, 0),
+    "fk_mimic_act_idx": (torch.int32, 0), "fk_topo_inv": (torch.int32, 0),
+    "sphere_link_idx": (torch.int32, 0), "sphere_local": (torch.float32, 3),
+    "sphere_radius": (torch.float32, 0),
+    "coarse_sphere_link_idx": (torch.int32, 0), "coarse_sphere_local": (torch.float32, 3),
+    "coarse_sphere_radius": (torch.float32, 0), "fine_link_offsets": (torch.int32, 0),
+    "coarse_self_pairs": (torch.int32, 2), "self_pair_ranges": (torch.int32, 2),
+}
+WORLD_SPEC = {
+    "world_spheres": (torch.float32, 4), "world_capsules": (torch.float32, 7),
+    "world_boxes": (torch.float32, 15), "world_halfspaces": (torch.float32, 6),
+    "self_pairs": (torch.int32, 2),
+}
+REQUIRED_KEYS = (
+    "fk_twists", "fk_parent_tf", "fk_parent_idx", "fk_act_idx", "fk_mimic_mul", "fk_mimic_off",
+    "fk_mimic_act_idx", "fk_topo_inv", "sphere_link_idx", "sphere_local", "sphere_radius",
+)
+
+
+def cuda_device(device=None) -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("prrtc_b200 requires a CUDA device (sm_100a); none is available")
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    d = torch.device(device)
+    if d.type != "cuda":
+        raise ValueError(f"prrtc_b200 runs on CUDA devices only, got {d}")
+    return d
+
+
+def as_tensor(x, dtype: torch.dtype, device: torch.device, cols: int = 0) -> torch.Tensor:
+    """Contiguous tensor of `dtype` on `device`; `cols` > 0 reshapes to (-1, cols)."""
+    if isinstance(x, torch.Tensor):
+        t = x.to(device=device, dtype=dtype)
+    else:
+        t = torch.as_tensor(np.asarray(x), dtype=dtype).to(device)
+    if cols:
+        t = t.reshape(-1, cols)
+    return t.contiguous()
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    if t is None or t.numel() == 0:
+        return None
+    return t.data_ptr()
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+class DeviceContext:
+    """collision_context tensors on one CUDA device."""
+
+    def __init__(self, ctx: dict | None, device: torch.device, world_keys: bool = True):
+        self.device = device
+        self.t: dict[str, torch.Tensor] = {}
+        spec = dict(ROBOT_SPEC)
+        if world_keys:
+            spec.update(WORLD_SPEC)
+        for k, (dt, cols) in spec.items():
+            if ctx is not None and k in ctx and ctx[k] is not None:
+                self.t[k] = as_tensor(ctx[k], dt, device, cols)
+            else:
+                self.t[k] = torch.zeros((0, cols) if cols else (0,), dtype=dt, device=device)
+
+    def n(self, key: str) -> int:
+        return int(self.t[key].shape[0])
+
+    def robot(self) -> _lib.Robot:
+        t = self.t
+        r = _lib.Robot()
+        for k in ("fk_twists", "fk_parent_tf", "fk_parent_idx", "fk_act_idx", "fk_mimic_mul", "fk_mimic_off",
+                  "fk_mimic_act_idx", "fk_topo_inv", "sphere_link_idx", "sphere_local", "sphere_radius",
+                  "coarse_sphere_link_idx", "coarse_sphere_local", "coarse_sphere_radius", "fine_link_offsets",
+                  "coarse_self_pairs", "self_pair_ranges"):
+            setattr(r, k, ptr(t[k]))
+        r.n_joints = self.n("fk_parent_idx")
+        r.n_spheres = self.n("sphere_link_idx")
+        nk = self.n("coarse_sphere_link_idx")
+        # the coarse model needs its K+1 fine offsets; otherwise it is absent
+        r.n_coarse = nk if self.n("fine_link_offsets") >= nk + 1 else 0
+        r.n_coarse_self_pairs = min(self.n("coarse_self_pairs"), self.n("self_pair_ranges")) if r.n_coarse else 0
+        return r
+
+    def world(self) -> _lib.World:
+        t = self.t
+        w = _lib.World()
+        for k in ("world_spheres", "world_capsules", "world_boxes", "world_halfspaces", "self_pairs"):
+            setattr(w, k, ptr(t[k]))
+        w.n_world_spheres = self.n("world_spheres")
+        w.n_world_capsules = self.n("world_capsules")
+        w.n_world_boxes = self.n("world_boxes")
+        w.n_world_halfspaces = self.n("world_halfspaces")
+        w.n_self_pairs = self.n("self_pairs")
+        return w
+
+
+def workspace(nbytes: int, device: torch.device) -> torch.Tensor:
+    # torch's CUDA allocator returns 512-byte aligned blocks
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def byref(s):
+    return C.byref(s)

@@ -1,0 +1,544 @@
+"""pRRTC planning API -- drop-in mirror of P-RRAX's ``cuda-rrtc/jax/prrtc.py``.
+
+Same function names, keyword arguments, defaults, validation and error
+behaviour as the reference (prrtc.py:255-585 ``prrtc_plan``, 882-1434
+``prrtc_plan_batch``, 1437-1508 ``prrtc_nearest_neighbor`` / ``prrtc_extend``),
+with torch tensors in place of jax arrays.  All computation runs in
+libprrtc_b200.so on the GPU; there is no CPU fallback.
+
+Differences from the reference, all deliberate:
+  * the host never blocks inside the planner call; scalars of the result are
+    read once at the end;
+  * the path is extracted by a device kernel (one read-back) instead of a
+    per-node device->host walk (prrtc.py:603-631);
+  * unused tree slots are NaN (the planner's "unwritten" sentinel), not 0;
+    consumers slice by tree size exactly as the reference's results do;
+  * extra keyword-only arguments: ``edge_resolution`` (raise the waypoints of an
+    edge to ceil(len/res)), ``threads_per_explorer``, ``waypoint_chunk``;
+    ``prrtc_plan_batch`` also takes ``goal_counts``, ``problem_order`` and
+    ``launch`` ("persistent" -- one persistent launch; "per_problem" -- one
+    planner launch per problem over a pool of streams, the reference's form).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import NamedTuple, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import REQUIRED_KEYS, DeviceContext, as_tensor, cuda_device, ptr, stream_handle, workspace
+
+_COLLISION_MODES = {"binary": 0, "differentiable": 1, "binary_coarse": 2, "binary_coarse_coop": 3}
+PATH_MAX_LEN = 16384
+
+
+class PRRTCResult(NamedTuple):
+    """Result of pRRTC planning (prrtc.py:31-45)."""
+
+    solved: bool
+    path: Optional[torch.Tensor]
+    tree_a_size: int
+    tree_b_size: int
+    iterations: int
+    cost: float
+    kernel_time_ms: Optional[float] = None
+    tree_a_configs: Optional[torch.Tensor] = None
+    tree_b_configs: Optional[torch.Tensor] = None
+    tree_a_parents: Optional[torch.Tensor] = None
+    tree_b_parents: Optional[torch.Tensor] = None
+
+
+def _resolve_collision_mode(collision_checker: str) -> int:
+    """prrtc.py:57-73."""
+    try:
+        return _COLLISION_MODES[collision_checker]
+    except KeyError:
+        if collision_checker == "robogpu":
+            raise ValueError(
+                "collision_checker='robogpu' is not available in the in-kernel planner: the point-cloud "
+                "checker runs host-driven. Use a host-driven planner loop with an external edge checker."
+            ) from None
+        raise ValueError(
+            f"collision_checker must be one of {sorted(_COLLISION_MODES)}, got {collision_checker!r}"
+        ) from None
+
+
+def _validate(step_size, granularity):
+    step_size = float(step_size)
+    if step_size <= 0.0:
+        raise ValueError("step_size must be > 0")
+    granularity = int(granularity)
+    if granularity < 1 or (granularity & (granularity - 1)) != 0:
+        raise ValueError(f"granularity must be a power of 2, got {granularity}")
+    if granularity > 64:
+        raise ValueError(f"granularity must be <= 64 (PRRTC_BLOCK_THREADS_MAX), got {granularity}")
+    return step_size, granularity
+
+
+def _check_context(collision_context, allow_unsafe_no_collision):
+    if collision_context is None and not allow_unsafe_no_collision:
+        raise ValueError(
+            "Collision-aware planning is the default. Provide collision_context "
+            "with required keys or set allow_unsafe_no_collision=True to opt out. "
+            f"Required keys: {REQUIRED_KEYS}"
+        )
+    if collision_context is not None:
+        missing = [k for k in REQUIRED_KEYS if k not in collision_context]
+        if missing:
+            raise ValueError(f"collision_context missing required keys: {missing}")
+
+
+def _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
+           dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin) -> _lib.Attrs:
+    a = _lib.Attrs()
+    a.max_iterations = int(min(max_iterations, 2**31 - 1))
+    a.step_size = float(step_size)
+    a.num_new_samples = int(num_new_samples)
+    a.balance_mode = int(balance_mode)
+    a.tree_ratio = float(tree_ratio)
+    a.dynamic_domain = 1 if dynamic_domain else 0
+    a.dd_alpha = float(dd_alpha)
+    a.dd_radius = float(dd_radius)
+    a.dd_min_radius = float(dd_min_radius)
+    a.dim = int(dim)
+    a.max_nodes = int(max_nodes)
+    a.granularity = int(granularity)
+    a.collision_mode = int(collision_mode)
+    a.collision_margin = float(collision_margin)
+    return a
+
+
+def _tuning(edge_resolution=0.0, threads_per_explorer=0, waypoint_chunk=0, resident_ctas=0) -> _lib.Tuning:
+    t = _lib.Tuning()
+    t.edge_resolution = float(edge_resolution or 0.0)
+    t.threads_per_explorer = int(threads_per_explorer or 0)
+    t.waypoint_chunk = int(waypoint_chunk or 0)
+    t.resident_ctas = int(resident_ctas or 0)
+    return t
+
+
+def _outputs_struct(ta, tb, pa, pb, sizes, completed, iters, conn, solved, ktime) -> _lib.Outputs:
+    o = _lib.Outputs()
+    o.tree_a_configs, o.tree_b_configs = ta.data_ptr(), tb.data_ptr()
+    o.tree_a_parents, o.tree_b_parents = pa.data_ptr(), pb.data_ptr()
+    o.tree_sizes, o.completed, o.iter_count = sizes.data_ptr(), completed.data_ptr(), iters.data_ptr()
+    o.connection_info, o.solved_flag, o.kernel_time_ms = conn.data_ptr(), solved.data_ptr(), ktime.data_ptr()
+    return o
+
+
+class _Results:
+    """Raw planner outputs of B problems plus device-extracted paths."""
+
+    def __init__(self, B: int, dim: int, N: int, device: torch.device, lead: tuple):
+        self.B, self.dim, self.N = B, dim, N
+        self.ta = torch.empty(lead + (dim, N), dtype=torch.float32, device=device)
+        self.tb = torch.empty(lead + (dim, N), dtype=torch.float32, device=device)
+        self.pa = torch.empty(lead + (N,), dtype=torch.int32, device=device)
+        self.pb = torch.empty(lead + (N,), dtype=torch.int32, device=device)
+        # scalars packed into one int32 block [B, 16] -> a single device->host copy
+        self.block = torch.zeros((B, 16), dtype=torch.int32, device=device)
+        self.sizes = torch.empty((B, 2), dtype=torch.int32, device=device)
+        self.completed = torch.empty((B, 2), dtype=torch.int32, device=device)
+        self.iters = torch.empty((B, 1), dtype=torch.int32, device=device)
+        self.conn = torch.empty((B, 3), dtype=torch.int32, device=device)
+        self.solved = torch.empty((B, 1), dtype=torch.int32, device=device)
+        self.ktime = torch.empty((B,), dtype=torch.float32, device=device)
+        self.max_len = int(min(PATH_MAX_LEN, 2 * N + 2))
+        self.paths = torch.empty((B, self.max_len, dim), dtype=torch.float32, device=device)
+        self.lengths = torch.empty((B,), dtype=torch.int32, device=device)
+        self.costs = torch.empty((B,), dtype=torch.float32, device=device)
+
+    def outputs(self) -> _lib.Outputs:
+        return _outputs_struct(self.ta, self.tb, self.pa, self.pb, self.sizes, self.completed, self.iters,
+                               self.conn, self.solved, self.ktime)
+
+    def extract(self, stream_ptr: int) -> None:
+        lib = _lib.load()
+        _lib.check(lib.prrtc_b200_extract_paths(self.B, self.dim, self.N, ptr(self.ta), ptr(self.tb), ptr(self.pa),
+                                                ptr(self.pb), ptr(self.conn), ptr(self.solved), self.max_len,
+                                                ptr(self.paths), ptr(self.lengths), ptr(self.costs), stream_ptr),
+                   "prrtc_b200_extract_paths")
+        b = self.block
+        b[:, 0:2] = self.sizes
+        b[:, 2:4] = self.completed
+        b[:, 4:5] = self.iters
+        b[:, 5:8] = self.conn
+        b[:, 8:9] = self.solved
+        b[:, 9] = self.ktime.view(torch.int32)
+        b[:, 10] = self.lengths
+        b[:, 11] = self.costs.view(torch.int32)
+
+    def to_results(self, trees: bool = True) -> list[PRRTCResult]:
+        host = self.block.cpu().numpy()
+        out = []
+        for i in range(self.B):
+            row = host[i]
+            solved = bool(row[8] == 1)
+            size_a, size_b = int(row[0]), int(row[1])
+            length = int(row[10])
+            kt = float(row[9:10].view(np.float32)[0])
+            cost = float(row[11:12].view(np.float32)[0]) if solved else float("inf")
+            path = None
+            if solved:
+                if length > 0:
+                    path = self.paths[i, :length]
+                else:  # longer than the device path buffer: walk on the host
+                    path = self._host_trace(i)
+                    cost = float(torch.linalg.norm(torch.diff(path, dim=0), dim=1).sum())
+            ta = self.ta[i] if self.ta.dim() == 3 else self.ta
+            tb = self.tb[i] if self.tb.dim() == 3 else self.tb
+            pa = self.pa[i] if self.pa.dim() == 2 else self.pa
+            pb = self.pb[i] if self.pb.dim() == 2 else self.pb
+            na, nb = min(size_a, self.N), min(size_b, self.N)
+            out.append(PRRTCResult(
+                solved=solved, path=path, tree_a_size=size_a, tree_b_size=size_b, iterations=int(row[4]),
+                cost=cost, kernel_time_ms=kt,
+                tree_a_configs=ta[:, :na] if trees else None, tree_b_configs=tb[:, :nb] if trees else None,
+                tree_a_parents=pa[:na] if trees else None, tree_b_parents=pb[:nb] if trees else None,
+            ))
+        return out
+
+    def _host_trace(self, i: int) -> torch.Tensor:
+        ta = (self.ta[i] if self.ta.dim() == 3 else self.ta).cpu()
+        tb = (self.tb[i] if self.tb.dim() == 3 else self.tb).cpu()
+        pa = (self.pa[i] if self.pa.dim() == 2 else self.pa).cpu().numpy()
+        pb = (self.pb[i] if self.pb.dim() == 2 else self.pb).cpu().numpy()
+        a, b = (int(x) for x in self.conn[i, :2].cpu())
+        nodes, curr = [], a
+        for _ in range(self.N):
+            nodes.append(ta[:, curr])
+            if pa[curr] == curr:
+                break
+            curr = int(pa[curr])
+        nodes.reverse()
+        curr = b
+        for _ in range(self.N):
+            nodes.append(tb[:, curr])
+            if pb[curr] == curr:
+                break
+            curr = int(pb[curr])
+        return torch.stack(nodes, 0).to(self.paths.device)
+
+
+def _limits(min_vals, max_vals, dim, device):
+    if min_vals is None:
+        min_vals = torch.full((dim,), -np.pi, dtype=torch.float32)
+    if max_vals is None:
+        max_vals = torch.full((dim,), np.pi, dtype=torch.float32)
+    return as_tensor(min_vals, torch.float32, device).reshape(dim), as_tensor(max_vals, torch.float32,
+                                                                             device).reshape(dim)
+
+
+def prrtc_plan(
+    start_config,
+    goal_configs,
+    max_iterations: int = 1_000_000,
+    step_size: float = 0.5,
+    num_new_samples: int = 128,
+    granularity: int = 16,
+    max_nodes: int = 1_000_000,
+    balance_mode: int = 1,
+    tree_ratio: float = 0.5,
+    dynamic_domain: bool = True,
+    dd_alpha: float = 1e-4,
+    dd_radius: float = 4.0,
+    dd_min_radius: float = 1.0,
+    min_vals=None,
+    max_vals=None,
+    collision_context: Optional[dict] = None,
+    allow_unsafe_no_collision: bool = False,
+    jit_trace: bool = False,
+    collision_checker: str = "binary",
+    collision_margin: float = 0.02,
+    *,
+    edge_resolution: float = 0.0,
+    threads_per_explorer: int = 0,
+    waypoint_chunk: int = 0,
+    device=None,
+) -> PRRTCResult:
+    """Plan one problem with the parallel bidirectional RRT-Connect planner (prrtc.py:255-585).
+
+    ``jit_trace`` is accepted for signature compatibility; the call is already a
+    single asynchronous C-ABI dispatch.
+    """
+    collision_mode = _resolve_collision_mode(collision_checker)
+    lib = _lib.load()
+    collision_margin = float(collision_margin)
+    start_shape = tuple(start_config.shape) if hasattr(start_config, "shape") else np.shape(start_config)
+    start_rows = 1 if len(start_shape) <= 1 else int(np.prod(start_shape[:-1]))
+    if start_rows != 1:
+        raise ValueError(
+            "prrtc_plan currently accepts a single start configuration per call. "
+            "For batches, call prrtc_plan_batch."
+        )
+    step_size, granularity = _validate(step_size, granularity)
+    _check_context(collision_context, allow_unsafe_no_collision)
+    dev = cuda_device(device)
+    start = as_tensor(start_config, torch.float32, dev).reshape(-1)
+    dim = int(start.shape[0])
+    goals = as_tensor(goal_configs, torch.float32, dev).reshape(-1, dim)
+    lo, hi = _limits(min_vals, max_vals, dim, dev)
+    ctx = DeviceContext(collision_context, dev)
+
+    inp = _lib.Inputs()
+    inp.start_config, inp.goal_configs, inp.num_goals = start.data_ptr(), goals.data_ptr(), goals.shape[0]
+    inp.min_vals, inp.max_vals = lo.data_ptr(), hi.data_ptr()
+    inp.robot, inp.world = ctx.robot(), ctx.world()
+    attrs = _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
+                   dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin)
+    tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk)
+    res = _Results(1, dim, int(max_nodes), dev, ())
+    ws = workspace(lib.prrtc_b200_plan_workspace_size(C.byref(inp), C.byref(attrs), C.byref(tun)), dev)
+    sp = stream_handle()
+    outs = res.outputs()
+    _lib.check(lib.prrtc_b200_plan(C.byref(inp), C.byref(outs), C.byref(attrs), C.byref(tun), ws.data_ptr(),
+                                   ws.numel(), sp), "prrtc_b200_plan")
+    res.extract(sp)
+    return res.to_results()[0]
+
+
+def _pack_worlds(contexts: Sequence[Optional[dict]], B: int):
+    """Padded [B, max_n, feat] world/self tensors + counts (prrtc.py:1009-1067)."""
+    specs = [("world_spheres", 4, np.float32), ("world_capsules", 7, np.float32), ("world_boxes", 15, np.float32),
+             ("world_halfspaces", 6, np.float32), ("self_pairs", 2, np.int32)]
+    packed, counts = {}, {}
+    for key, feat, dt in specs:
+        arrs = []
+        for i, c in enumerate(contexts):
+            if c is None or key not in c or c[key] is None:
+                a = np.zeros((0, feat), dtype=dt)
+            else:
+                a = np.asarray(c[key], dtype=dt)
+                if a.ndim != 2 or a.shape[1] != feat:
+                    raise ValueError(f"collision_context[{i}]['{key}'] must have shape (N, {feat}), got {a.shape}")
+            arrs.append(a)
+        n = np.array([a.shape[0] for a in arrs], dtype=np.int32)
+        m = int(n.max()) if B else 0
+        p = np.zeros((B, m, feat), dtype=dt)
+        for i, a in enumerate(arrs):
+            p[i, : a.shape[0]] = a
+        packed[key], counts[key] = p, n
+    return packed, counts
+
+
+def lpt_order(contexts: Sequence[Optional[dict]], goal_counts=None) -> np.ndarray:
+    """Longest-processing-time order: problems with the most collision work first."""
+    cost = []
+    for c in contexts:
+        if c is None:
+            cost.append(0.0)
+            continue
+        ns = sum(int(np.asarray(c.get(k, np.zeros((0,)))).shape[0]) * w
+                 for k, w in (("world_spheres", 1.0), ("world_capsules", 2.0), ("world_boxes", 3.0),
+                              ("world_halfspaces", 1.0)))
+        cost.append(ns)
+    return np.argsort(-np.asarray(cost), kind="stable").astype(np.int32)
+
+
+def prrtc_plan_batch(
+    start_configs,
+    goal_configs,
+    max_iterations: int = 1_000_000,
+    step_size: float = 0.5,
+    num_new_samples: int = 128,
+    granularity: int = 16,
+    max_nodes: int = 1_000_000,
+    balance_mode: int = 1,
+    tree_ratio: float = 0.5,
+    dynamic_domain: bool = True,
+    dd_alpha: float = 1e-4,
+    dd_radius: float = 4.0,
+    dd_min_radius: float = 1.0,
+    min_vals=None,
+    max_vals=None,
+    collision_context=None,
+    allow_unsafe_no_collision: bool = False,
+    jit_trace: bool = False,
+    collision_checker: str = "binary",
+    collision_margin: float = 0.02,
+    *,
+    goal_counts=None,
+    problem_order="auto",
+    launch: str = "persistent",
+    edge_resolution: float = 0.0,
+    threads_per_explorer: int = 0,
+    waypoint_chunk: int = 0,
+    resident_ctas: int = 0,
+    return_trees: bool = True,
+    device=None,
+) -> list[PRRTCResult]:
+    """Plan B independent problems (prrtc.py:882-1434).
+
+    ``collision_context`` is one dict shared by every problem, or a list/tuple of
+    per-problem dicts (robot tables from the first non-None entry; worlds and
+    self pairs packed into padded tensors with counts).
+    """
+    lib = _lib.load()
+    collision_mode = _resolve_collision_mode(collision_checker)
+    step_size, granularity = _validate(step_size, granularity)
+    if collision_context is None:
+        _check_context(None, allow_unsafe_no_collision)
+    dev = cuda_device(device)
+    starts = as_tensor(start_configs, torch.float32, dev)
+    if starts.dim() == 1:
+        starts = starts.reshape(1, -1)
+    B, dim = int(starts.shape[0]), int(starts.shape[1])
+    goals = as_tensor(goal_configs, torch.float32, dev)
+    if goals.dim() == 2:
+        goals = goals[:, None, :]
+    if goals.dim() != 3 or goals.shape[0] != B:
+        raise ValueError(f"goal_configs must have shape (batch, num_goals, dim), got {tuple(goals.shape)} "
+                         f"with batch_size={B}")
+    goals = goals.contiguous()
+    G = int(goals.shape[1])
+    lo, hi = _limits(min_vals, max_vals, dim, dev)
+
+    per_problem = isinstance(collision_context, (list, tuple))
+    if per_problem:
+        if len(collision_context) != B:
+            raise ValueError("When collision_context is a list/tuple, it must have length "
+                             f"equal to batch_size ({B}), got {len(collision_context)}")
+        contexts = list(collision_context)
+        first = next((c for c in contexts if c is not None), None)
+        if first is None:
+            _check_context(None, allow_unsafe_no_collision)
+        else:
+            for i, c in enumerate(contexts):
+                if c is not None:
+                    missing = [k for k in REQUIRED_KEYS if k not in c]
+                    if missing:
+                        raise ValueError(f"collision_context[{i}] missing required keys: {missing}")
+    else:
+        _check_context(collision_context, allow_unsafe_no_collision)
+        contexts = [collision_context] * B
+        first = collision_context
+
+    robot_ctx = DeviceContext(first, dev, world_keys=not per_problem)
+    bi = _lib.BatchInputs()
+    bi.batch = B
+    bi.start_configs, bi.goal_configs, bi.num_goals = starts.data_ptr(), goals.data_ptr(), G
+    keep = []
+    if goal_counts is not None:
+        gc = as_tensor(goal_counts, torch.int32, dev).reshape(B)
+        keep.append(gc)
+        bi.goal_counts = gc.data_ptr()
+    bi.min_vals, bi.max_vals = lo.data_ptr(), hi.data_ptr()
+    bi.robot = robot_ctx.robot()
+    if per_problem and first is not None:
+        packed, counts = _pack_worlds(contexts, B)
+        for key, field in (("world_spheres", "world_spheres"), ("world_capsules", "world_capsules"),
+                           ("world_boxes", "world_boxes"), ("world_halfspaces", "world_halfspaces"),
+                           ("self_pairs", "self_pairs")):
+            t = torch.from_numpy(packed[key]).to(dev)
+            c = torch.from_numpy(counts[key]).to(dev)
+            keep += [t, c]
+            setattr(bi, field, ptr(t))
+            setattr(bi, "max_" + field, int(packed[key].shape[1]))
+            setattr(bi, field + "_count", ptr(c))
+    elif first is not None:
+        w = robot_ctx.world()
+        bi.world_spheres, bi.max_world_spheres = w.world_spheres, w.n_world_spheres
+        bi.world_capsules, bi.max_world_capsules = w.world_capsules, w.n_world_capsules
+        bi.world_boxes, bi.max_world_boxes = w.world_boxes, w.n_world_boxes
+        bi.world_halfspaces, bi.max_world_halfspaces = w.world_halfspaces, w.n_world_halfspaces
+        bi.self_pairs, bi.max_self_pairs = w.self_pairs, w.n_self_pairs
+    order = None
+    if isinstance(problem_order, str):
+        if problem_order == "auto" and per_problem:
+            order = lpt_order(contexts)
+    elif problem_order is not None:
+        order = np.asarray(problem_order, dtype=np.int32).reshape(B)
+    if order is not None:
+        ot = torch.from_numpy(np.ascontiguousarray(order)).to(dev)
+        keep.append(ot)
+        bi.problem_order = ot.data_ptr()
+
+    attrs = _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
+                   dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin)
+    tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk, resident_ctas)
+    res = _Results(B, dim, int(max_nodes), dev, (B,))
+    sp = stream_handle()
+    if launch == "persistent":
+        ws = workspace(lib.prrtc_b200_plan_batch_workspace_size(C.byref(bi), C.byref(attrs), C.byref(tun)), dev)
+        outs = res.outputs()
+        _lib.check(lib.prrtc_b200_plan_batch(C.byref(bi), C.byref(outs), C.byref(attrs), C.byref(tun),
+                                             ws.data_ptr(), ws.numel(), sp), "prrtc_b200_plan_batch")
+    elif launch == "per_problem":
+        _plan_per_problem(lib, bi, res, attrs, tun, contexts, robot_ctx, starts, goals, goal_counts, lo, hi, dev)
+    else:
+        raise ValueError(f"launch must be 'persistent' or 'per_problem', got {launch!r}")
+    res.extract(sp)
+    return res.to_results(trees=return_trees)
+
+
+def _plan_per_problem(lib, bi, res, attrs, tun, contexts, robot_ctx, starts, goals, goal_counts, lo, hi, dev,
+                      n_streams: int = 8):
+    """One plain planner launch per problem over a pool of streams (the reference's
+    batch handlers launch each problem on its own child stream, prrtc_planner.cu:1785-1900)."""
+    B, dim, G = int(starts.shape[0]), int(starts.shape[1]), int(goals.shape[1])
+    main = torch.cuda.current_stream()
+    streams = [torch.cuda.Stream(device=dev) for _ in range(min(n_streams, B))]
+    ev = torch.cuda.Event()
+    ev.record(main)
+    gcs = None if goal_counts is None else np.asarray(goal_counts).reshape(B)
+    keep = []
+    for i in range(B):
+        s = streams[i % len(streams)]
+        s.wait_event(ev)
+        ctx = DeviceContext(contexts[i], dev) if contexts[i] is not None else DeviceContext(None, dev)
+        keep.append(ctx)
+        inp = _lib.Inputs()
+        inp.start_config = starts[i].data_ptr()
+        ng = G if gcs is None else max(1, min(int(gcs[i]), G))
+        inp.goal_configs, inp.num_goals = goals[i].data_ptr(), ng
+        inp.min_vals, inp.max_vals = lo.data_ptr(), hi.data_ptr()
+        inp.robot, inp.world = ctx.robot(), ctx.world()
+        outs = _outputs_struct(res.ta[i], res.tb[i], res.pa[i], res.pb[i], res.sizes[i], res.completed[i],
+                               res.iters[i], res.conn[i], res.solved[i], res.ktime[i:i + 1])
+        ws = workspace(lib.prrtc_b200_plan_workspace_size(C.byref(inp), C.byref(attrs), C.byref(tun)), dev)
+        ws.record_stream(s)
+        keep.append(ws)
+        _lib.check(lib.prrtc_b200_plan(C.byref(inp), C.byref(outs), C.byref(attrs), C.byref(tun), ws.data_ptr(),
+                                       ws.numel(), s.cuda_stream), "prrtc_b200_plan")
+    for s in streams:
+        main.wait_stream(s)
+    torch.cuda.current_stream().synchronize()
+
+
+def prrtc_nearest_neighbor(tree_configs, query_configs, tree_size):
+    """Nearest tree node of each query (prrtc.py:1437-1469).  Returns (distances, indices)."""
+    lib = _lib.load()
+    dev = cuda_device(tree_configs.device if isinstance(tree_configs, torch.Tensor) else None)
+    tree = as_tensor(tree_configs, torch.float32, dev)
+    q = as_tensor(query_configs, torch.float32, dev)
+    dim, N = int(tree.shape[0]), int(tree.shape[1])
+    q = q.reshape(-1, dim)
+    B = int(q.shape[0])
+    ts = as_tensor(np.array([int(tree_size)], dtype=np.int32), torch.int32, dev)
+    idx = torch.empty((B,), dtype=torch.int32, device=dev)
+    dist = torch.empty((B,), dtype=torch.float32, device=dev)
+    ws = workspace(lib.prrtc_b200_nearest_neighbor_workspace_size(B), dev)
+    _lib.check(lib.prrtc_b200_nearest_neighbor(ptr(tree), dim, N, ptr(ts), ptr(q), B, ptr(idx), ptr(dist),
+                                               ws.data_ptr(), ws.numel(), stream_handle()),
+               "prrtc_b200_nearest_neighbor")
+    return dist, idx
+
+
+def prrtc_extend(tree_configs, nearest_indices, samples, step_size):
+    """Step-limited extend (prrtc.py:1472-1508).  Returns (new_configs, parent_indices, valid_flags)."""
+    lib = _lib.load()
+    dev = cuda_device(tree_configs.device if isinstance(tree_configs, torch.Tensor) else None)
+    tree = as_tensor(tree_configs, torch.float32, dev)
+    dim, N = int(tree.shape[0]), int(tree.shape[1])
+    ni = as_tensor(nearest_indices, torch.int32, dev).reshape(-1)
+    s = as_tensor(samples, torch.float32, dev).reshape(-1, dim)
+    B = int(s.shape[0])
+    st = as_tensor(np.array([step_size], dtype=np.float32), torch.float32, dev)
+    out = torch.empty((B, dim), dtype=torch.float32, device=dev)
+    par = torch.empty((B,), dtype=torch.int32, device=dev)
+    valid = torch.empty((B,), dtype=torch.int32, device=dev)
+    _lib.check(lib.prrtc_b200_extend(ptr(tree), dim, N, ptr(ni), ptr(s), B, ptr(st), ptr(out), ptr(par),
+                                     ptr(valid), stream_handle()), "prrtc_b200_extend")
+    return out, par, valid

@@ -1,0 +1,95 @@
+"""C-ABI surface: the library loads, exports every function include/prrtc_b200.h
+declares, and rejects malformed arguments before any CUDA call (no GPU needed)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared():
+    text = (ROOT / "include" / "prrtc_b200.h").read_text()
+    return sorted(set(re.findall(r"\b(prrtc_b200_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    for must in ("prrtc_b200_plan", "prrtc_b200_plan_batch", "prrtc_b200_nearest_neighbor", "prrtc_b200_extend",
+                 "prrtc_b200_check_configs", "prrtc_b200_extract_paths", "prrtc_b200_smooth_cost_grad"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from prrtc_b200 import _lib
+
+    lib = _lib.load()
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_lib.EXPORTS) <= set(declared())
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    from prrtc_b200 import _lib
+
+    lib = _lib.load()
+    a = _lib.Attrs()
+    a.dim, a.max_nodes, a.step_size, a.num_new_samples, a.granularity = 7, 1024, 0.5, 8, 16
+    inp, out = _lib.Inputs(), _lib.Outputs()
+    # null outputs / inputs
+    assert lib.prrtc_b200_plan(C.byref(inp), C.byref(out), C.byref(a), None, None, 0, None) == _lib.EARG
+    bad = _lib.Attrs.from_buffer_copy(a)
+    bad.granularity = 12
+    assert lib.prrtc_b200_plan(C.byref(inp), C.byref(out), C.byref(bad), None, None, 0, None) == _lib.EARG
+    bad = _lib.Attrs.from_buffer_copy(a)
+    bad.step_size = 0.0
+    assert lib.prrtc_b200_plan(C.byref(inp), C.byref(out), C.byref(bad), None, None, 0, None) == _lib.EARG
+    bad = _lib.Attrs.from_buffer_copy(a)
+    bad.dim = 17
+    assert lib.prrtc_b200_plan(C.byref(inp), C.byref(out), C.byref(bad), None, None, 0, None) == _lib.EUNSUPPORTED
+    assert lib.prrtc_b200_nearest_neighbor(None, 7, 10, None, None, 4, None, None, None, 0, None) == _lib.EARG
+    assert lib.prrtc_b200_error_string(_lib.EWORKSPACE).decode().startswith("workspace")
+
+
+def test_workspace_sizes_are_host_arithmetic():
+    from prrtc_b200 import _lib
+
+    lib = _lib.load()
+    a = _lib.Attrs()
+    a.dim, a.max_nodes = 7, 65536
+    inp = _lib.Inputs()
+    inp.robot.n_joints, inp.robot.n_spheres = 7, 56
+    inp.world.n_world_spheres, inp.world.n_self_pairs = 16, 960
+    n1 = lib.prrtc_b200_plan_workspace_size(C.byref(inp), C.byref(a), None)
+    a.max_nodes = 4096
+    n2 = lib.prrtc_b200_plan_workspace_size(C.byref(inp), C.byref(a), None)
+    # radii for two trees dominate: 2 * max_nodes floats
+    assert n1 - n2 == 2 * (65536 - 4096) * 4
+    assert lib.prrtc_b200_nearest_neighbor_workspace_size(100) >= 800
+
+
+def test_api_validation_matches_reference_errors():
+    import numpy as np
+
+    import prrtc_b200 as P
+
+    start, goal = np.zeros(7, np.float32), np.ones((1, 7), np.float32)
+    with pytest.raises(ValueError, match="step_size"):
+        P.prrtc_plan(start, goal, step_size=0.0, allow_unsafe_no_collision=True)
+    with pytest.raises(ValueError, match="power of 2"):
+        P.prrtc_plan(start, goal, granularity=12, allow_unsafe_no_collision=True)
+    with pytest.raises(ValueError, match="<= 64"):
+        P.prrtc_plan(start, goal, granularity=128, allow_unsafe_no_collision=True)
+    with pytest.raises(ValueError, match="robogpu"):
+        P.prrtc_plan(start, goal, collision_checker="robogpu")
+    with pytest.raises(ValueError, match="collision_checker must be one of"):
+        P.prrtc_plan(start, goal, collision_checker="sdf")
+    with pytest.raises(ValueError, match="Collision-aware planning is the default"):
+        P.prrtc_plan(start, goal)
+    with pytest.raises(ValueError, match="missing required keys"):
+        P.prrtc_plan(start, goal, collision_context={"fk_twists": np.zeros((1, 6))})
+    with pytest.raises(ValueError, match="single start configuration"):
+        P.prrtc_plan(np.zeros((2, 7)), goal, allow_unsafe_no_collision=True)

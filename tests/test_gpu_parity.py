@@ -1,0 +1,296 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the oracle and against
+the reference's own device code compiled from its sources (oracle/_ref)."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import make_problem
+
+pytestmark = pytest.mark.gpu
+
+REF_LIB = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "libprrtc_ref.so"
+
+
+def _ref():
+    if not REF_LIB.exists():
+        pytest.skip("reference harness oracle/_ref/libprrtc_ref.so not built (needs the reference sources)")
+    lib = C.CDLL(str(REF_LIB))
+    P, I, F = C.c_void_p, C.c_int, C.c_float
+    lib.ref_halton_samples.argtypes = [I, I, I, P, P, P, P]
+    lib.ref_prime_order.argtypes = [I, P, P]
+    lib.ref_step.argtypes = [P, I, I, I, P, P, I, F, I, P, P, P, P, P, P]
+    lib.ref_connect.argtypes = [P, I, I, P, F, I, F, P, P, P]
+    lib.ref_nn.argtypes = [P, I, I, I, P, I, P, P, P]
+    lib.ref_extend.argtypes = [P, P, P, F, I, I, I, P, P, P, P]
+    return lib
+
+
+def _bits(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32)).view(np.uint32)
+
+
+def _s():
+    return torch.cuda.current_stream().cuda_stream
+
+
+@pytest.mark.parametrize("dim", [7, 14])
+def test_halton_bit_exact(cuda, orc, dim):
+    from prrtc_b200.collision import halton_samples
+
+    lo = np.full(dim, -2.8, np.float32)
+    hi = np.full(dim, 2.8, np.float32)
+    for e in (0, 1, 5, 63, 127, 255):
+        mine = halton_samples(e, 300, lo, hi).cpu().numpy()
+        ora = orc.halton_samples(e, 300, lo, hi)
+        assert np.array_equal(_bits(mine), _bits(ora)), f"explorer {e}"
+
+
+def test_reference_sampler_pins_oracle(cuda, orc):
+    ref = _ref()
+    for dim in (7, 14):
+        lo = torch.full((dim,), -2.8, device=cuda)
+        hi = torch.linspace(1.0, 3.0, dim, device=cuda)
+        for e in (0, 1, 2, 17, 127, 255):
+            out = torch.empty((257, dim), device=cuda)
+            assert ref.ref_halton_samples(e, 257, dim, lo.data_ptr(), hi.data_ptr(), out.data_ptr(), _s()) == 0
+            po = torch.empty(16, dtype=torch.int32, device=cuda)
+            assert ref.ref_prime_order(e, po.data_ptr(), _s()) == 0
+            ora = orc.halton_samples(e, 257, lo.cpu().numpy(), hi.cpu().numpy())
+            assert np.array_equal(po.cpu().numpy(), orc.prime_order(e))
+            assert np.array_equal(_bits(out.cpu().numpy()), _bits(ora)), f"explorer {e} dim {dim}"
+
+
+def _random_tree(rng, dim, N, n):
+    t = np.full((dim, N), np.nan, np.float32)
+    t[:, :n] = rng.uniform(-2.8, 2.8, (dim, n)).astype(np.float32)
+    return t
+
+
+@pytest.mark.parametrize("block", [16, 64])
+def test_reference_step_pins_oracle(cuda, orc, block):
+    """NN + extend + waypoints of the reference planner (842-904) vs the oracle."""
+    ref = _ref()
+    rng = np.random.default_rng(3)
+    dim, N = 7, 4096
+    for trial in range(20):
+        n = int(rng.integers(1, N))
+        tree = _random_tree(rng, dim, N, n)
+        sample = rng.uniform(-2.8, 2.8, dim).astype(np.float32)
+        radii = np.full(N, np.finfo(np.float32).max, np.float32)
+        tt = torch.from_numpy(tree).to(cuda)
+        out_d = torch.empty(1, device=cuda)
+        out_i = torch.empty(1, dtype=torch.int32, device=cuda)
+        out_s = torch.empty(1, dtype=torch.int32, device=cuda)
+        out_c = torch.empty(dim, device=cuda)
+        out_w = torch.empty((block, dim), device=cuda)
+        step = 0.5 if trial % 2 else 10.0
+        ts, tr = torch.from_numpy(sample).to(cuda), torch.from_numpy(radii).to(cuda)
+        rc = ref.ref_step(tt.data_ptr(), N, dim, n, ts.data_ptr(), tr.data_ptr(), 1, step, block, out_d.data_ptr(),
+                          out_i.data_ptr(), out_s.data_ptr(), out_c.data_ptr(), out_w.data_ptr(), _s())
+        assert rc == 0
+        idx, dsq = orc.nearest(tree, n, sample)
+        assert int(out_i.item()) == idx
+        assert _bits(out_d.cpu().numpy())[0] == _bits([dsq])[0]
+        assert out_s.item() == 0
+        cand = orc.extend(tree[:, idx], sample, float(np.sqrt(np.float32(dsq))), step)
+        assert np.array_equal(_bits(out_c.cpu().numpy()), _bits(cand))
+        wps = orc.edge_waypoints(tree[:, idx], cand, block)
+        assert np.array_equal(_bits(out_w.cpu().numpy()), _bits(wps))
+
+
+def test_reference_connect_pins_oracle(cuda, orc):
+    ref = _ref()
+    rng = np.random.default_rng(5)
+    dim, N = 7, 256
+    for _ in range(50):
+        tree = _random_tree(rng, dim, N, N)
+        cand = rng.uniform(-2.8, 2.8, dim).astype(np.float32)
+        cidx, cdsq = orc.nearest(tree, N, cand)
+        step = float(rng.choice([0.1, 0.5, 1.0]))
+        n_ext = torch.empty(1, dtype=torch.int32, device=cuda)
+        vec = torch.empty(dim, device=cuda)
+        tt, tc = torch.from_numpy(tree).to(cuda), torch.from_numpy(cand).to(cuda)
+        assert ref.ref_connect(tt.data_ptr(), N, dim, tc.data_ptr(), cdsq, cidx, step,
+                               n_ext.data_ptr(), vec.data_ptr(), _s()) == 0
+        cd = np.sqrt(np.float32(cdsq), dtype=np.float32)
+        ne = int(np.ceil(np.float32(cd) / np.float32(step))) if cd > 1e-8 else 0
+        assert n_ext.item() == ne
+        want = ((tree[:, cidx] - cand) / np.float32(ne)).astype(np.float32) if ne else np.zeros(dim, np.float32)
+        assert np.array_equal(_bits(vec.cpu().numpy()), _bits(want))
+
+
+def test_nearest_neighbor_matches_oracle_and_reference(cuda, orc):
+    from prrtc_b200 import prrtc_nearest_neighbor
+
+    rng = np.random.default_rng(7)
+    for dim, N, n in ((7, 65536, 50000), (14, 8192, 8192), (3, 4099, 4000)):
+        tree = _random_tree(rng, dim, N, n)
+        q = rng.uniform(-2.8, 2.8, (64, dim)).astype(np.float32)
+        tt, tq = torch.from_numpy(tree).to(cuda), torch.from_numpy(q).to(cuda)
+        dist, idx = prrtc_nearest_neighbor(tt, tq, n)
+        oi, od = orc.nearest_batch(tree, n, q)
+        assert np.array_equal(idx.cpu().numpy(), oi)
+        assert np.array_equal(_bits(dist.cpu().numpy()), _bits(np.sqrt(od.astype(np.float32))))
+        if REF_LIB.exists():
+            ref = _ref()
+            ri = torch.empty(64, dtype=torch.int32, device=cuda)
+            rd = torch.empty(64, device=cuda)
+            assert ref.ref_nn(tt.data_ptr(), dim, N, n, tq.data_ptr(), 64, ri.data_ptr(),
+                              rd.data_ptr(), _s()) == 0
+            assert np.array_equal(ri.cpu().numpy(), oi)  # random floats: no ties
+            assert np.array_equal(_bits(rd.cpu().numpy()), _bits(dist.cpu().numpy()))
+
+
+def test_nearest_neighbor_ties_lowest_index(cuda, orc):
+    from prrtc_b200 import prrtc_nearest_neighbor
+
+    dim, N = 7, 8192
+    rng = np.random.default_rng(11)
+    base = rng.uniform(-1, 1, (dim, 37)).astype(np.float32)
+    tree = np.tile(base, (1, N // 37 + 1))[:, :N].copy()
+    q = base[:, [3, 5, 36]].T.copy()
+    dist, idx = prrtc_nearest_neighbor(torch.from_numpy(tree).to(cuda), torch.from_numpy(q).to(cuda), N)
+    assert idx.cpu().tolist() == [3, 5, 36]
+    assert np.all(dist.cpu().numpy() == 0.0)
+    oi, _ = orc.nearest_batch(tree, N, q)
+    assert oi.tolist() == [3, 5, 36]
+
+
+def test_extend_matches_reference(cuda, orc):
+    from prrtc_b200 import prrtc_extend
+
+    rng = np.random.default_rng(13)
+    dim, N = 7, 1024
+    tree = _random_tree(rng, dim, N, N)
+    ni = rng.integers(0, N, 100).astype(np.int32)
+    s = rng.uniform(-2.8, 2.8, (100, dim)).astype(np.float32)
+    tt, tn, tsm = torch.from_numpy(tree).to(cuda), torch.from_numpy(ni).to(cuda), torch.from_numpy(s).to(cuda)
+    out, par, valid = prrtc_extend(tt, tn, tsm, 0.5)
+    assert np.array_equal(par.cpu().numpy(), ni) and np.all(valid.cpu().numpy() == 1)
+    if REF_LIB.exists():
+        ref = _ref()
+        ro = torch.empty((100, dim), device=cuda)
+        rp = torch.empty(100, dtype=torch.int32, device=cuda)
+        rv = torch.empty(100, dtype=torch.int32, device=cuda)
+        assert ref.ref_extend(tt.data_ptr(), tn.data_ptr(), tsm.data_ptr(), 0.5, dim, N, 100, ro.data_ptr(), rp.data_ptr(),
+                              rv.data_ptr(), _s()) == 0
+        assert np.array_equal(_bits(ro.cpu().numpy()), _bits(out.cpu().numpy()))
+
+
+def _rot_angle(Ra, Rb):
+    """Rotation angle between two rotation matrices, well conditioned near 0:
+    |Ra - Rb|_F = 2 sqrt(2) sin(theta / 2)."""
+    s = np.linalg.norm(Ra - Rb) / (2.0 * np.sqrt(2.0))
+    return float(2.0 * np.arcsin(min(1.0, s)))
+
+
+@pytest.mark.parametrize("robot", ["arm", "dual"])
+def test_fk_within_1e5_of_f64(cuda, orc, robot, arm, dual):
+    from prrtc_b200.collision import forward_kinematics
+    from prrtc_b200.context import build_collision_context
+
+    rob = arm if robot == "arm" else dual
+    ctx = build_collision_context(rob, None)
+    rng = np.random.default_rng(17)
+    q = rng.uniform(rob.lower, rob.upper, (500, rob.dim)).astype(np.float32)
+    F = forward_kinematics(q, ctx).cpu().numpy()
+    sc = orc.Scene(ctx, rob.dim)
+    worst_t = worst_r = 0.0
+    for i in range(q.shape[0]):
+        ref = sc.fk(q[i].astype(np.float64))
+        for k in range(ref.shape[0]):
+            worst_t = max(worst_t, float(np.abs(F[i, k, 9:] - ref[k, 9:]).max()))
+            worst_r = max(worst_r, _rot_angle(F[i, k, :9].reshape(3, 3).astype(np.float64), ref[k, :9].reshape(3, 3)))
+    assert worst_t < 1e-5, worst_t
+    assert worst_r < 1e-5, worst_r
+
+
+WORLDS = ["spheres16", "tabletop", "uneven", "large"]
+
+
+@pytest.mark.parametrize("kind", WORLDS)
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_collision_verdicts_match_oracle(cuda, orc, kind, mode):
+    from prrtc_b200.collision import CollisionChecker
+
+    pr = make_problem(kind, 1)
+    ctx = pr.context
+    rng = np.random.default_rng(19)
+    q = rng.uniform(pr.lower, pr.upper, (3000, pr.dim)).astype(np.float32)
+    names = ["binary", "differentiable", "binary_coarse", "binary_coarse_coop"]
+    chk = CollisionChecker(ctx, pr.dim, names[mode], 0.02)
+    mine = chk.check(q).cpu().numpy()
+    sweep = chk.check(q, full_sweep=True).cpu().numpy()
+    assert np.array_equal(mine, sweep)
+    sc = orc.Scene(ctx, pr.dim)
+    ora = sc.check_configs(q, mode, 0.02)
+    md = sc.min_distances(q)
+    thr = 0.02 if mode == 1 else 0.0
+    far = np.abs(md - thr) > 1e-4
+    assert far.mean() > 0.95
+    assert np.array_equal(mine[far], ora[far]), f"{(mine[far] != ora[far]).sum()} verdicts differ"
+    assert 0.02 < mine.mean() < 0.999
+
+
+def _check_tree_sound(sc, tree, parents, size, dim, sample=200):
+    n = min(size, tree.shape[1])
+    idx = np.linspace(0, n - 1, min(n, sample)).astype(int)
+    nodes = tree[:, idx].T
+    assert not np.isnan(nodes).any()
+    d = sc.min_distances(nodes)
+    assert (d > -2e-3).all(), d.min()
+    assert (parents[:n] >= 0).all() and (parents[:n] < n).all()
+
+
+@pytest.mark.parametrize("kind,seed,checker", [("spheres16", 0, "binary"), ("spheres16", 1, "binary_coarse_coop"),
+                                               ("tabletop", 2, "binary_coarse"), ("tabletop", 3, "differentiable"),
+                                               ("uneven", 4, "binary_coarse_coop")])
+def test_plan_solves_and_revalidates(cuda, orc, kind, seed, checker):
+    from prrtc_b200 import prrtc_plan
+
+    pr = make_problem(kind, seed)
+    r = prrtc_plan(pr.start, pr.goals, max_iterations=5000, num_new_samples=64, max_nodes=65536,
+                   min_vals=pr.lower, max_vals=pr.upper, collision_context=pr.context, collision_checker=checker,
+                   edge_resolution=0.01)
+    assert r.solved
+    path = r.path.cpu().numpy()
+    assert np.array_equal(path[0], pr.start)
+    assert any(np.array_equal(path[-1], g) for g in pr.goals)
+    sc = orc.Scene(pr.context, pr.dim)
+    ok, md = sc.validate_path(path, 0.01)
+    assert ok, md
+    assert abs(r.cost - float(np.linalg.norm(np.diff(path, axis=0), axis=1).sum())) < 1e-3
+    assert r.kernel_time_ms > 0.0
+    _check_tree_sound(sc, r.tree_a_configs.cpu().numpy(), r.tree_a_parents.cpu().numpy(), r.tree_a_size, pr.dim)
+    _check_tree_sound(sc, r.tree_b_configs.cpu().numpy(), r.tree_b_parents.cpu().numpy(), r.tree_b_size, pr.dim)
+
+
+@pytest.mark.parametrize("launch", ["persistent", "per_problem"])
+def test_batch_uneven_solves(cuda, orc, launch):
+    from prrtc_b200 import prrtc_plan_batch
+
+    probs = [make_problem("uneven", 100 + i) for i in range(12)]
+    G = max(p.goals.shape[0] for p in probs)
+    dim = probs[0].dim
+    goals = np.zeros((len(probs), G, dim), np.float32)
+    for i, p in enumerate(probs):
+        goals[i, : p.goals.shape[0]] = p.goals
+    res = prrtc_plan_batch(np.stack([p.start for p in probs]), goals, max_iterations=5000, num_new_samples=32,
+                           max_nodes=16384, min_vals=probs[0].lower, max_vals=probs[0].upper,
+                           collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
+                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01, launch=launch)
+    assert len(res) == len(probs)
+    assert sum(r.solved for r in res) >= len(probs) - 1
+    for p, r in zip(probs, res):
+        if not r.solved:
+            continue
+        path = r.path.cpu().numpy()
+        assert np.array_equal(path[0], p.start)
+        assert any(np.array_equal(path[-1], g) for g in p.goals)
+        ok, md = orc.Scene(p.context, dim).validate_path(path, 0.01)
+        assert ok, md
