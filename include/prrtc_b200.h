@@ -133,6 +133,9 @@ typedef struct {
     int32_t threads_per_explorer;/* CTA size of one explorer: 64, 128 or 256 (default 128) */
     int32_t waypoint_chunk;      /* waypoints checked per CTA pass: 8, 16 or 32 (default 16) */
     int32_t resident_ctas;       /* batched planner grid (default: all resident CTAs) */
+    uint64_t* stats;             /* optional device counters [4], accumulated: edges checked,
+                                    configurations checked, FP32 flops of the collision work
+                                    executed, nearest-neighbour nodes scanned */
 } prrtc_tuning_t;
 
 size_t prrtc_b200_plan_workspace_size(const prrtc_inputs_t* in, const prrtc_attrs_t* attrs,
@@ -228,6 +231,11 @@ int prrtc_b200_smooth_cost_grad(const prrtc_robot_t* robot, const prrtc_world_t*
                                 const float* waypoints, int32_t n_paths, int32_t n_waypoints,
                                 float margin, float beta, float w_len, float* cost, float* grad,
                                 void* workspace, size_t workspace_bytes, void* stream);
+
+/* Diagnostic: FP32 FFMA throughput probe (blocks x threads, iters x 8 independent
+ * FFMA chains per thread); sink receives one value per block so the work is live.
+ * Used to measure the FP32 roofline denominator. */
+int prrtc_b200_fp32_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink, void* stream);
 
 const char* prrtc_b200_error_string(int code);
 int prrtc_b200_last_cuda_error(void);

@@ -67,7 +67,7 @@ class Attrs(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [
         ("edge_resolution", F32), ("threads_per_explorer", I32), ("waypoint_chunk", I32),
-        ("resident_ctas", I32),
+        ("resident_ctas", I32), ("stats", P),
     ]
 
 
@@ -92,6 +92,7 @@ EXPORTS = (
     "prrtc_b200_check_configs_workspace_size", "prrtc_b200_check_configs",
     "prrtc_b200_fk", "prrtc_b200_halton", "prrtc_b200_extract_paths",
     "prrtc_b200_smooth_workspace_size", "prrtc_b200_smooth_cost_grad",
+    "prrtc_b200_fp32_probe",
     "prrtc_b200_error_string", "prrtc_b200_last_cuda_error", "prrtc_b200_version",
 )
 
@@ -110,6 +111,7 @@ _SIGS = {
     "prrtc_b200_extract_paths": (C.c_int, [I32, I32, I32, P, P, P, P, P, P, I32, P, P, P, P]),
     "prrtc_b200_smooth_workspace_size": (C.c_size_t, [P, P]),
     "prrtc_b200_smooth_cost_grad": (C.c_int, [P, P, I32, P, I32, I32, F32, F32, F32, P, P, P, C.c_size_t, P]),
+    "prrtc_b200_fp32_probe": (C.c_int, [I32, I32, I32, P, P]),
     "prrtc_b200_error_string": (C.c_char_p, [C.c_int]),
     "prrtc_b200_last_cuda_error": (C.c_int, []),
     "prrtc_b200_version": (C.c_int, []),

@@ -82,16 +82,18 @@ static PackSrc make_pack(const prrtc_robot_t& r, const prrtc_world_t& w, int dim
 struct Tuned {
     float edge_res;
     int threads, cw, resident;
+    unsigned long long* stats;
 };
 
 static Tuned tuned(const prrtc_tuning_t* t) {
-    Tuned o{0.0f, 128, 16, 0};
+    Tuned o{0.0f, 128, 16, 0, nullptr};
     if (t) {
         if (t->edge_resolution > 0.0f) o.edge_res = t->edge_resolution;
         if (t->threads_per_explorer == 64 || t->threads_per_explorer == 128 || t->threads_per_explorer == 256)
             o.threads = t->threads_per_explorer;
         if (t->waypoint_chunk == 8 || t->waypoint_chunk == 16 || t->waypoint_chunk == 32) o.cw = t->waypoint_chunk;
         if (t->resident_ctas > 0) o.resident = t->resident_ctas;
+        o.stats = reinterpret_cast<unsigned long long*>(t->stats);
     }
     return o;
 }
@@ -108,6 +110,7 @@ static void fill_launch(PlanLaunch& L, const prrtc_outputs_t* out, const prrtc_a
     L.granularity = a->granularity; L.step = a->step_size; L.tree_ratio = a->tree_ratio;
     L.dd_alpha = a->dd_alpha; L.dd_radius = a->dd_radius; L.dd_min_radius = a->dd_min_radius;
     L.edge_res = tu.edge_res; L.threads = tu.threads; L.cw = tu.cw; L.resident = tu.resident;
+    L.stats = tu.stats;
 }
 
 static bool outputs_ok(const prrtc_outputs_t* o) {
@@ -344,6 +347,12 @@ int prrtc_b200_smooth_cost_grad(const prrtc_robot_t* robot, const prrtc_world_t*
     if (e != cudaSuccess) return cuda_fail(e);
     e = launch_smooth(blob, world->self_pairs, s.J, s.S, dim, waypoints, n_paths, n_waypoints, margin, beta, w_len,
                       cost, grad, nullptr, st);
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
+int prrtc_b200_fp32_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink, void* stream) {
+    if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || !sink) return PRRTC_B200_EARG;
+    cudaError_t e = launch_fp32_probe(blocks, threads, iters, sink, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 

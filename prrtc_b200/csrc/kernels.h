@@ -54,6 +54,7 @@ struct PlanLaunch {
     // tuning
     int threads, cw, resident;
     int persistent;
+    unsigned long long* stats;         // optional device counters (kStat*)
 };
 
 size_t plan_workspace_bytes(int B, int N, size_t blob_stride);
@@ -85,6 +86,8 @@ cudaError_t launch_smooth(const unsigned char* blob, const int32_t* pairs, int J
                           const float* wp, int P, int W, float margin, float beta, float w_len, float* cost,
                           float* grad, float* scratch, cudaStream_t st);
 size_t smooth_scratch_bytes(int J, int S, int P, int W);
+
+cudaError_t launch_fp32_probe(int blocks, int threads, int iters, float* sink, cudaStream_t st);
 
 int device_sm_count();
 size_t device_max_smem();

@@ -412,6 +412,7 @@ __device__ int choose_tree(int mode, int local_iter, int bid, int nblocks, int s
 __device__ bool cta_edge_collides(const Scene& sc, const CcBufs& B, const float* base, const float* delta, int dim,
                                   int G, int CW) {
     const int tid = threadIdx.x, T = blockDim.x;
+    if (B.stats && tid == 0) atomicAdd(&B.stats[kStatEdges], 1ull);
     for (int c0 = 0; c0 < G; c0 += CW) {
         const int nw = min(CW, G - c0);
         for (int i = tid; i < nw * dim; i += T) {
@@ -465,6 +466,7 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
         const int t = X.t, o = 1 - t;
         cta_nearest(P.tree[t], N, dim, X.n_t, X.sample, X.red_d, X.red_i);
         if (tid == 0) {
+            if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_t);
             const int nn = X.red_i[0];
             int skip = nn == INT_MAX;
             if (!skip) {
@@ -513,6 +515,7 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
         // connect (prrtc_planner.cu:949-1043)
         cta_nearest(P.tree[o], N, dim, X.n_o, X.cand, X.red_d, X.red_i);
         if (tid == 0) {
+            if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_o);
             const int cnn = X.red_i[0];
             int n_ext = 0;
             if (cnn != INT_MAX) {
@@ -585,7 +588,8 @@ __global__ void __launch_bounds__(256) explore_kernel(PlanLaunch L) {
     const int tid = threadIdx.x;
     const bool staged = L.blob_cap > 0;
     unsigned char* blob_sm = dsm;
-    const CcBufs B = cc_bufs(dsm + (staged ? L.blob_cap : 0), L.J, L.S, L.K, L.Q, L.cw);
+    CcBufs B = cc_bufs(dsm + (staged ? L.blob_cap : 0), L.J, L.S, L.K, L.Q, L.cw);
+    B.stats = L.stats;
     if (tid == 0) mbar_init(&mbar);
     __syncthreads();
     uint32_t phase = 0;

@@ -286,4 +286,28 @@ cudaError_t launch_halton(int explorer, int n, int dim, const float* lo, const f
     return cudaGetLastError();
 }
 
+// ============================================================================ FP32 probe
+
+// 8 independent FFMA chains per thread: the FP32 pipe stays busy without
+// dependency stalls.  2 * 8 * iters flops per thread.
+__global__ void fp32_probe_kernel(int iters, float* sink) {
+    float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
+    float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
+    const float m = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    const float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 12345.0f) sink[blockIdx.x] = r;  // never true; keeps the chains live
+}
+
+cudaError_t launch_fp32_probe(int blocks, int threads, int iters, float* sink, cudaStream_t st) {
+    fp32_probe_kernel<<<blocks, threads, 0, st>>>(iters, sink);
+    return cudaGetLastError();
+}
+
 }  // namespace prrtc

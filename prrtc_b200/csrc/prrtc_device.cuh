@@ -30,6 +30,18 @@ constexpr int kSphChunk = 8;     // fine spheres held in registers per work item
 constexpr int kPairChunk = 32;   // explicit self pairs per work item
 constexpr float kFar = 1.0e18f;  // centre of a sphere that can never collide
 
+// FP32 operations per primitive test as issued by the functions below (FFMA = 2,
+// FADD/FMUL = 1; min/max/abs and the MUFU of sin/cos/sqrt are not counted).
+constexpr int kFlopSphere = 10, kFlopCapsule = 22, kFlopBox = 27, kFlopHalfspace = 6;
+constexpr int kFlopPair = 10, kFlopPairExplicit = 11;
+constexpr int kFlopXform = 18;                  // one sphere centre
+constexpr int kFlopJointLocal = 90, kFlopJointChain = 63;
+
+// Device counters of the collision work (optional): [0] edges checked,
+// [1] configurations checked, [2] FP32 flops executed by primitive tests,
+// transforms and FK, [3] nearest-neighbour nodes scanned.
+enum { kStatEdges = 0, kStatConfigs = 1, kStatFlops = 2, kStatNnNodes = 3, kStatCount = 4 };
+
 // ----------------------------------------------------------------------------- blob
 
 struct BlobHeader {
@@ -363,52 +375,62 @@ __device__ __forceinline__ bool hit_halfspace(float4 c, float4 h) {
 }
 
 // One obstacle chunk of one type against up to 8 sphere centres held in registers.
-// Returns true on the first hit unless full_sweep.
+// Returns true on the first hit unless full_sweep; n_done = obstacles tested,
+// flop = FP32 operations of one (sphere, obstacle) test of this chunk's type.
 __device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int och, const float4 (&s)[kSphChunk],
-                                                     bool full_sweep) {
+                                                     bool full_sweep, int& n_done, int& flop) {
     const BlobHeader& h = *sc.h;
     int c = och;
     bool hit = false;
+    n_done = 0;
     const int ns = cdiv(h.Ns, kObsChunk), nc = cdiv(h.Nc, kObsChunk), nb = cdiv(h.Nb, kObsChunk);
     if (c < ns) {
+        flop = kFlopSphere;
         const int o0 = c * kObsChunk, o1 = min(h.Ns, o0 + kObsChunk);
         for (int o = o0; o < o1; ++o) {
             const float4 ob = sc.ws[o];
 #pragma unroll
             for (int k = 0; k < kSphChunk; ++k) hit |= hit_sphere(s[k], ob);
+            ++n_done;
             if (hit && !full_sweep) return true;
         }
         return hit;
     }
     c -= ns;
     if (c < nc) {
+        flop = kFlopCapsule;
         const int o0 = c * kObsChunk, o1 = min(h.Nc, o0 + kObsChunk);
         for (int o = o0; o < o1; ++o) {
             const float4 p = sc.wc[2 * o], d = sc.wc[2 * o + 1];
 #pragma unroll
             for (int k = 0; k < kSphChunk; ++k) hit |= hit_capsule(s[k], p, d);
+            ++n_done;
             if (hit && !full_sweep) return true;
         }
         return hit;
     }
     c -= nc;
     if (c < nb) {
+        flop = kFlopBox;
         const int o0 = c * kObsChunk, o1 = min(h.Nb, o0 + kObsChunk);
         for (int o = o0; o < o1; ++o) {
             const float4 b0 = sc.wb[4 * o], a1 = sc.wb[4 * o + 1], a2 = sc.wb[4 * o + 2], a3 = sc.wb[4 * o + 3];
 #pragma unroll
             for (int k = 0; k < kSphChunk; ++k) hit |= hit_box(s[k], b0, a1, a2, a3);
+            ++n_done;
             if (hit && !full_sweep) return true;
         }
         return hit;
     }
     c -= nb;
     {
+        flop = kFlopHalfspace;
         const int o0 = c * kObsChunk, o1 = min(h.Nh, o0 + kObsChunk);
         for (int o = o0; o < o1; ++o) {
             const float4 hs = sc.wh[o];
 #pragma unroll
             for (int k = 0; k < kSphChunk; ++k) hit |= hit_halfspace(s[k], hs);
+            ++n_done;
             if (hit && !full_sweep) return true;
         }
     }
@@ -426,6 +448,7 @@ struct CcBufs {
     uint32_t* dirty; // [CW][KW]
     uint32_t* gate;  // [CW][QW]
     uint32_t* hit;   // [1]
+    unsigned long long* stats;  // optional device counters (kStat*), may be null
 };
 
 __host__ __device__ inline int cc_smem_bytes(int J, int S, int K, int Q, int CW) {
@@ -454,6 +477,7 @@ __device__ inline CcBufs cc_bufs(unsigned char* base, int J, int S, int K, int Q
     b.dirty = reinterpret_cast<uint32_t*>(p); p += align16(CW * KW * 4);
     b.gate = reinterpret_cast<uint32_t*>(p);  p += align16(CW * QW * 4);
     b.hit = reinterpret_cast<uint32_t*>(p);
+    b.stats = nullptr;
     return b;
 }
 
@@ -520,6 +544,7 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
         }
     }
     __syncthreads();
+    unsigned long long flops = 0;
     // D: coarse pre-pass -> dirty groups and touching coarse self pairs
     if (gated) {
         const int n_cw = nw * K * h.n_och;
@@ -532,7 +557,9 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
                 s[0] = B.cctr[w * K + k];
 #pragma unroll
                 for (int m = 1; m < kSphChunk; ++m) s[m] = make_float4(kFar, kFar, kFar, 0.0f);
-                if (obstacles_vs_spheres(sc, och, s, false)) atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
+                int nd, fl;
+                if (obstacles_vs_spheres(sc, och, s, false, nd, fl)) atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
+                flops += (unsigned long long)nd * fl;
             } else {
                 const int r = it - n_cw;
                 const int qq = r / nw, w = r - qq * nw;
@@ -542,6 +569,7 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
                 const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
                 const float t = a.w + b.w - inflate;
                 if (fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= t * t) atomicOr(&B.gate[w * QW + (qq >> 5)], 1u << (qq & 31));
+                flops += kFlopPairExplicit;
             }
         }
         __syncthreads();
@@ -565,7 +593,9 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
 #pragma unroll
             for (int m = 0; m < kSphChunk; ++m)
                 s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : make_float4(kFar, kFar, kFar, 0.0f);
-            hit = obstacles_vs_spheres(sc, och, s, full_sweep);
+            int nd, fl;
+            hit = obstacles_vs_spheres(sc, och, s, full_sweep, nd, fl);
+            flops += (unsigned long long)nd * fl * ch.y;
         } else {
             const int r = it - n_world;
             const int ii = r / nw;
@@ -582,12 +612,14 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
                     a[m] = (m < na) ? C[item.x + m] : make_float4(kFar, kFar, kFar, 0.0f);
                     a[m].w -= inflate;
                 }
-                for (int bb = 0; bb < nb; ++bb) {
+                int bb = 0;
+                for (; bb < nb; ++bb) {
                     const float4 b = C[item.y + bb];
 #pragma unroll
                     for (int m = 0; m < kSphChunk; ++m) hit |= hit_sphere(a[m], b);
-                    if (hit && !full_sweep) break;
+                    if (hit && !full_sweep) { ++bb; break; }
                 }
+                flops += (unsigned long long)bb * na * kFlopPair;
             } else {  // explicit pairs [p0, p0+count) of the pair list (global memory)
                 const int p1 = min(item.x + item.z, h.P);
                 for (int p = item.x; p < p1; ++p) {
@@ -597,11 +629,23 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
                     const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
                     const float t = a.w + b.w - inflate;
                     hit |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= t * t;
+                    flops += kFlopPairExplicit;
                     if (hit && !full_sweep) break;
                 }
             }
         }
         if (hit) atomicOr(B.hit, 1u << w);
+    }
+    if (B.stats) {
+        if (tid == 0) {
+            unsigned long long fk = (unsigned long long)nw * (J * (kFlopJointLocal + kFlopJointChain) + S * kFlopXform);
+            if (gated) fk += (unsigned long long)nw * K * kFlopXform;
+            flops += fk;
+            atomicAdd(&B.stats[kStatConfigs], (unsigned long long)nw);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) flops += __shfl_xor_sync(0xffffffffu, flops, off);
+        if ((tid & 31) == 0 && flops) atomicAdd(&B.stats[kStatFlops], flops);
     }
     __syncthreads();
     return *vhit;
