@@ -77,13 +77,15 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
     for (int i = tid; i < S; i += T) {
         sph[i] = make_float4(s.sloc[i * 3], s.sloc[i * 3 + 1], s.sloc[i * 3 + 2], s.srad[i]);
         const int li = s.sli[i];
-        sfr[i] = (li >= 0 && li < J) ? (s.topo_inv ? s.topo_inv[li] : li) : -1;
+        int f = (li >= 0 && li < J) ? (s.topo_inv ? s.topo_inv[li] : li) : -1;
+        sfr[i] = (f >= 0 && f < J) ? f : -1;
     }
     float4* grp = reinterpret_cast<float4*>(blob + L.o_grp);
     for (int k = tid; k < K; k += T) {
         grp[2 * k] = make_float4(s.cloc[k * 3], s.cloc[k * 3 + 1], s.cloc[k * 3 + 2], s.crad[k]);
         const int li = s.cli[k];
-        const int f = (li >= 0 && li < J) ? (s.topo_inv ? s.topo_inv[li] : li) : -1;
+        int f = (li >= 0 && li < J) ? (s.topo_inv ? s.topo_inv[li] : li) : -1;
+        if (f >= J) f = -1;
         const int s0 = s.foff ? clampi(s.foff[k], 0, S) : 0;
         const int s1 = s.foff ? clampi(s.foff[k + 1], 0, S) : 0;
         grp[2 * k + 1] = make_float4(__int_as_float(f), __int_as_float(s0), __int_as_float(s1), 0.0f);

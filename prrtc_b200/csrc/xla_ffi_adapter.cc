@@ -1,0 +1,148 @@
+// xla_ffi_adapter.cc -- XLA FFI handlers exporting the reference's six symbols
+// (PrrtcPlannerFfi, PrrtcPlannerBatchFfi, PrrtcPlannerBatchCtxFfi,
+// PrrtcNearestNeighborFfi, PrrtcExtendFfi, PrrtcIterationFfi; registered by
+// cuda-rrtc/jax/prrtc.py:141-146) on top of the C-ABI in include/prrtc_b200.h.
+//
+// Compiled only where jaxlib provides xla/ffi/api/ffi.h (prrtc_b200/build.py
+// adds -DPRRTC_WITH_XLA_FFI and jaxlib's include directory).  The binding order,
+// names and dtypes are the reference's interface contract
+// (cuda-rrtc/CUDA/prrtc_planner.cu:1946-2117, prrtc_nearest_neighbor.cu:132-141,
+// prrtc_extend.cu:129-140).  Unlike the reference handlers these never block the
+// host and allocate only when their per-device workspace must grow.
+#if defined(PRRTC_WITH_XLA_FFI)
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <vector>
+
+#include "../../include/prrtc_b200.h"
+#include "xla/ffi/api/ffi.h"
+
+namespace ffi = xla::ffi;
+
+namespace {
+
+// Per-device workspace that only grows (allocation happens outside any steady
+// state: the first call of a given size).
+struct Pool {
+    std::mutex m;
+    std::vector<void*> ptr;
+    std::vector<size_t> bytes;
+    void* get(size_t need, cudaError_t* err) {
+        int dev = 0;
+        *err = cudaGetDevice(&dev);
+        if (*err != cudaSuccess) return nullptr;
+        std::lock_guard<std::mutex> lock(m);
+        if ((int)ptr.size() <= dev) { ptr.resize(dev + 1, nullptr); bytes.resize(dev + 1, 0); }
+        if (bytes[dev] < need) {
+            if (ptr[dev]) cudaFree(ptr[dev]);
+            ptr[dev] = nullptr;
+            bytes[dev] = 0;
+            *err = cudaMalloc(&ptr[dev], need);
+            if (*err != cudaSuccess) return nullptr;
+            bytes[dev] = need;
+        }
+        return ptr[dev];
+    }
+};
+Pool g_pool;
+
+template <typename B>
+int rows(const B& b) { return b.dimensions().size() == 0 ? 0 : static_cast<int>(b.dimensions()[0]); }
+
+ffi::Error status(int rc) {
+    if (rc == PRRTC_B200_OK) return ffi::Error::Success();
+    const ffi::ErrorCode code = rc == PRRTC_B200_EARG ? ffi::ErrorCode::kInvalidArgument : ffi::ErrorCode::kInternal;
+    return ffi::Error(code, prrtc_b200_error_string(rc));
+}
+
+using F32 = ffi::Buffer<ffi::DataType::F32>;
+using S32 = ffi::Buffer<ffi::DataType::S32>;
+using RF32 = ffi::Result<ffi::Buffer<ffi::DataType::F32>>;
+using RS32 = ffi::Result<ffi::Buffer<ffi::DataType::S32>>;
+
+prrtc_robot_t robot_of(F32 tw, F32 ptf, S32 par, S32 act, F32 mm, F32 mo, S32 mact, S32 topo, S32 sli, F32 sloc,
+                       F32 srad, S32 cli, F32 cloc, F32 crad, S32 foff, S32 cpairs, S32 cranges) {
+    prrtc_robot_t r{};
+    r.fk_twists = tw.typed_data(); r.fk_parent_tf = ptf.typed_data(); r.fk_parent_idx = par.typed_data();
+    r.fk_act_idx = act.typed_data(); r.fk_mimic_mul = mm.typed_data(); r.fk_mimic_off = mo.typed_data();
+    r.fk_mimic_act_idx = mact.typed_data(); r.fk_topo_inv = topo.typed_data(); r.n_joints = rows(par);
+    r.sphere_link_idx = sli.typed_data(); r.sphere_local = sloc.typed_data(); r.sphere_radius = srad.typed_data();
+    r.n_spheres = rows(sli);
+    const int k = rows(cli);
+    r.coarse_sphere_link_idx = cli.typed_data(); r.coarse_sphere_local = cloc.typed_data();
+    r.coarse_sphere_radius = crad.typed_data();
+    r.fine_link_offsets = rows(foff) >= k + 1 ? foff.typed_data() : nullptr;
+    r.n_coarse = r.fine_link_offsets ? k : 0;
+    r.coarse_self_pairs = cpairs.typed_data(); r.self_pair_ranges = cranges.typed_data();
+    r.n_coarse_self_pairs = r.n_coarse ? rows(cpairs) : 0;
+    return r;
+}
+
+prrtc_attrs_t attrs_of(int max_iterations, float step_size, int num_new_samples, int balance_mode, float tree_ratio,
+                       int dynamic_domain, float dd_alpha, float dd_radius, float dd_min_radius, int dim,
+                       int max_nodes, int granularity, int collision_mode, float collision_margin) {
+    prrtc_attrs_t a{};
+    a.max_iterations = max_iterations; a.step_size = step_size; a.num_new_samples = num_new_samples;
+    a.balance_mode = balance_mode; a.tree_ratio = tree_ratio; a.dynamic_domain = dynamic_domain;
+    a.dd_alpha = dd_alpha; a.dd_radius = dd_radius; a.dd_min_radius = dd_min_radius; a.dim = dim;
+    a.max_nodes = max_nodes; a.granularity = granularity; a.collision_mode = collision_mode;
+    a.collision_margin = collision_margin;
+    return a;
+}
+
+ffi::Error PlannerImpl(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi, F32 tw, F32 ptf, S32 par, S32 act,
+                       F32 mm, F32 mo, S32 mact, S32 topo, S32 sli, F32 sloc, F32 srad, F32 ws, F32 wc, F32 wb, F32 wh,
+                       S32 sp, S32 cli, F32 cloc, F32 crad, S32 foff, S32 cpairs, S32 cranges, RF32 ta, RF32 tb,
+                       RS32 pa, RS32 pb, RS32 sizes, RS32 completed, RS32 iters, RS32 conn, RS32 solved, RF32 ktime,
+                       int max_iterations, float step_size, int num_new_samples, int balance_mode, float tree_ratio,
+                       int dynamic_domain, float dd_alpha, float dd_radius, float dd_min_radius, int dim,
+                       int max_nodes, int granularity, int collision_mode, float collision_margin) {
+    prrtc_inputs_t in{};
+    in.start_config = start.typed_data();
+    in.goal_configs = goals.typed_data();
+    in.num_goals = rows(goals);
+    in.min_vals = lo.typed_data();
+    in.max_vals = hi.typed_data();
+    in.robot = robot_of(tw, ptf, par, act, mm, mo, mact, topo, sli, sloc, srad, cli, cloc, crad, foff, cpairs, cranges);
+    in.world.world_spheres = ws.typed_data(); in.world.n_world_spheres = rows(ws);
+    in.world.world_capsules = wc.typed_data(); in.world.n_world_capsules = rows(wc);
+    in.world.world_boxes = wb.typed_data(); in.world.n_world_boxes = rows(wb);
+    in.world.world_halfspaces = wh.typed_data(); in.world.n_world_halfspaces = rows(wh);
+    in.world.self_pairs = sp.typed_data(); in.world.n_self_pairs = rows(sp);
+    prrtc_outputs_t out{ta->typed_data(), tb->typed_data(), pa->typed_data(), pb->typed_data(),
+                        sizes->typed_data(), completed->typed_data(), iters->typed_data(), conn->typed_data(),
+                        solved->typed_data(), ktime->typed_data()};
+    const prrtc_attrs_t a = attrs_of(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio,
+                                     dynamic_domain, dd_alpha, dd_radius, dd_min_radius, dim, max_nodes, granularity,
+                                     collision_mode, collision_margin);
+    const size_t need = prrtc_b200_plan_workspace_size(&in, &a, nullptr);
+    cudaError_t e;
+    void* w = g_pool.get(need, &e);
+    if (!w) return ffi::Error(ffi::ErrorCode::kInternal, cudaGetErrorString(e));
+    return status(prrtc_b200_plan(&in, &out, &a, nullptr, w, need, stream));
+}
+
+}  // namespace
+
+#define PRRTC_PLANNER_BINDING                                                                          \
+    ffi::Ffi::Bind()                                                                                   \
+        .Ctx<ffi::PlatformStream<cudaStream_t>>()                                                      \
+        .Arg<F32>().Arg<F32>().Arg<F32>().Arg<F32>()                /* start, goals, min, max */       \
+        .Arg<F32>().Arg<F32>().Arg<S32>().Arg<S32>()                /* twists, parent_tf, parent, act */ \
+        .Arg<F32>().Arg<F32>().Arg<S32>().Arg<S32>()                /* mimic mul/off/act, topo_inv */  \
+        .Arg<S32>().Arg<F32>().Arg<F32>()                           /* sphere link/local/radius */     \
+        .Arg<F32>().Arg<F32>().Arg<F32>().Arg<F32>().Arg<S32>()     /* world x4, self_pairs */         \
+        .Arg<S32>().Arg<F32>().Arg<F32>().Arg<S32>().Arg<S32>().Arg<S32>() /* coarse model */          \
+        .Ret<F32>().Ret<F32>().Ret<S32>().Ret<S32>().Ret<S32>().Ret<S32>().Ret<S32>().Ret<S32>()       \
+        .Ret<S32>().Ret<F32>()                                                                         \
+        .Attr<int>("max_iterations").Attr<float>("step_size").Attr<int>("num_new_samples")            \
+        .Attr<int>("balance_mode").Attr<float>("tree_ratio").Attr<int>("dynamic_domain")              \
+        .Attr<float>("dd_alpha").Attr<float>("dd_radius").Attr<float>("dd_min_radius")                \
+        .Attr<int>("dim").Attr<int>("max_nodes").Attr<int>("granularity").Attr<int>("collision_mode")  \
+        .Attr<float>("collision_margin")
+
+XLA_FFI_DEFINE_HANDLER_SYMBOL(PrrtcPlannerFfi, PlannerImpl, PRRTC_PLANNER_BINDING);
+
+#endif  // PRRTC_WITH_XLA_FFI
