@@ -42,6 +42,7 @@ extern "C" {
 #define PRRTC_B200_EWORKSPACE (-2)  /* workspace missing, too small or misaligned */
 #define PRRTC_B200_ECUDA (-3)       /* a CUDA runtime call failed (prrtc_b200_last_cuda_error) */
 #define PRRTC_B200_EUNSUPPORTED (-4)/* shape outside the supported limits */
+#define PRRTC_B200_ETOOLARGE (-5)   /* scene larger than the no-allocation scene buffer */
 
 #define PRRTC_B200_DIM_MAX 16        /* CONFIG_DIM_MAX, prrtc_helpers.cuh:10 */
 #define PRRTC_B200_MAX_JOINTS 64     /* PRRTC_MAX_JOINTS, prrtc_planner.cu:31-33 */
@@ -201,6 +202,25 @@ int prrtc_b200_check_configs(const prrtc_robot_t* robot, const prrtc_world_t* wo
                              const float* configs, int32_t n, int32_t collision_mode,
                              float collision_margin, int32_t full_sweep, int32_t* verdicts,
                              void* workspace, size_t workspace_bytes, void* stream);
+
+/* Same verdicts as prrtc_b200_check_configs, with no workspace and no
+ * allocation of any kind.  No counterpart in the reference: it serves callers
+ * that cannot call cudaMalloc or provide scratch memory (work issued while
+ * another library captures the stream into a CUDA graph, real-time loops that
+ * forbid allocation after start-up, plug-in hosts without access to an
+ * allocator).  The packed scene goes to a file-scope device array of
+ * PRRTC_B200_NOALLOC_SCENE_MAX bytes that every GPU loading the library holds
+ * until process exit; a larger scene returns PRRTC_B200_ETOOLARGE before any
+ * CUDA call.  The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress) with that device current, so make that first call
+ * before any stream capture.  Every call rewrites the whole array; calls that
+ * overlap on the GPU (other streams or host threads on the same device) share
+ * it and race -- serialise them. */
+#define PRRTC_B200_NOALLOC_SCENE_MAX (256 * 1024)
+int prrtc_b200_check_configs_noalloc(const prrtc_robot_t* robot, const prrtc_world_t* world, int32_t dim,
+                                     const float* configs, int32_t n, int32_t collision_mode,
+                                     float collision_margin, int32_t full_sweep, int32_t* verdicts,
+                                     void* stream);
 
 /* Forward kinematics: frames [n,n_joints,12] (row-major R then t) in output
  * frame order. */

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "../../include/prrtc_b200.h"
 #include "kernels.h"
@@ -132,6 +133,8 @@ const char* prrtc_b200_error_string(int code) {
         case PRRTC_B200_EWORKSPACE: return "workspace missing, too small or not 256-byte aligned";
         case PRRTC_B200_ECUDA: return cudaGetErrorString((cudaError_t)g_last_cuda);
         case PRRTC_B200_EUNSUPPORTED: return "shape outside the supported limits";
+        case PRRTC_B200_ETOOLARGE:
+            return "scene larger than the no-allocation scene buffer (PRRTC_B200_NOALLOC_SCENE_MAX bytes)";
         default: return "unknown error";
     }
 }
@@ -347,6 +350,61 @@ int prrtc_b200_smooth_cost_grad(const prrtc_robot_t* robot, const prrtc_world_t*
     if (e != cudaSuccess) return cuda_fail(e);
     e = launch_smooth(blob, world->self_pairs, s.J, s.S, dim, waypoints, n_paths, n_waypoints, margin, beta, w_len,
                       cost, grad, nullptr, st);
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
+// ---------------------------------------------------------------------------
+// Collision check without allocation.  Some callers cannot call cudaMalloc or
+// hand out scratch memory -- code running while another library captures the
+// stream into a CUDA graph, real-time control loops that forbid allocation once
+// started, plug-in hosts whose allocator is not reachable from the calling
+// thread.  For them the packed scene lives in this file-scope device array.
+// Every GPU that loads the library holds the array until the process exits.
+// Each call rewrites the array completely (the pack kernel writes the header
+// and every section the checker reads), so nothing has to be cleared between
+// calls; calls that overlap on the GPU (different streams, or different host
+// threads on one device) share the array and race.
+static __device__ __align__(256) unsigned char g_noalloc_scene[PRRTC_B200_NOALLOC_SCENE_MAX];
+
+static std::mutex g_noalloc_mutex;
+static unsigned char* g_noalloc_ptr[256];  // device address of g_noalloc_scene, per device ordinal
+
+// Host code cannot use g_noalloc_scene's name as a device address: resolve it
+// once per device, with that device current.
+static int noalloc_scene_ptr(unsigned char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (dev < 0 || dev >= 256) return PRRTC_B200_EUNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scene);
+        if (e != cudaSuccess) return cuda_fail(e);
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return PRRTC_B200_OK;
+}
+
+int prrtc_b200_check_configs_noalloc(const prrtc_robot_t* robot, const prrtc_world_t* world, int32_t dim,
+                                     const float* configs, int32_t n, int32_t mode, float margin,
+                                     int32_t full_sweep, int32_t* verdicts, void* stream) {
+    if (n == 0) return PRRTC_B200_OK;
+    if (!robot || !world || !configs || !verdicts || n < 0 || mode < 0 || mode > 3) return PRRTC_B200_EARG;
+    if (dim < 1 || dim > PRRTC_B200_DIM_MAX) return PRRTC_B200_EUNSUPPORTED;
+    int rc = check_robot(*robot);
+    if (rc) return rc;
+    const PackSrc s = make_pack(*robot, *world, dim, mode, margin);
+    const size_t stride = blob_stride(s);
+    if (stride > (size_t)PRRTC_B200_NOALLOC_SCENE_MAX) return PRRTC_B200_ETOOLARGE;
+    unsigned char* blob = nullptr;
+    if ((rc = noalloc_scene_ptr(&blob))) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = launch_pack(s, 1, blob, stride, st);
+    if (e != cudaSuccess) return cuda_fail(e);
+    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, configs, n, full_sweep, verdicts,
+                     st);
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 
