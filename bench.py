@@ -276,13 +276,13 @@ def run_ours(a):
     lib = _lib.load()
     problems = make_workload(a.problems, rank, gpu_checker(dev))
     settings = PlanSettings()
-    from prrtc_b200.autotune import choose_samples
+    from prrtc_b200.autotune import choose
 
     buckets = bucket_problems(problems)
-    tuned = {N: choose_samples(ps, N, settings, dev) for N, ps in buckets.items()}
+    tuned = {N: choose(ps, N, settings, dev) for N, ps in buckets.items()}
     planners = {}
     for N, ps in buckets.items():
-        s = PlanSettings(**{**settings.__dict__, "num_new_samples": tuned[N]})
+        s = PlanSettings(**{**settings.__dict__, **tuned[N]})
         planners[N] = BatchPlanner(ps, N, s, dev)
     flush = torch.empty(int(256 * 2**20) // 4, dtype=torch.float32, device=dev)
 
@@ -349,7 +349,7 @@ def run_ours(a):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "problems_per_gpu": len(problems),
                    "buckets": {str(N): len(ps) for N, ps in buckets.items()},
-                   "num_new_samples": {str(N): v for N, v in tuned.items()},
+                   "tuned": {str(N): v for N, v in tuned.items()},
                    "collision_checker": settings.collision_checker, "edge_resolution": settings.edge_resolution,
                    "threads_per_explorer": settings.threads_per_explorer, "l2": "flushed (256 MB write) between steps",
                    "launch": "eager" if a.eager else "one CUDA graph per bucket",
@@ -390,7 +390,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
     flops = cfgs = edges = nn_nodes = 0
     ms = 0.0
     for N, pl in planners.items():
-        s = PlanSettings(**{**settings.__dict__, "num_new_samples": tuned[N]})
+        s = PlanSettings(**{**settings.__dict__, **tuned[N]})
         ip = BatchPlanner(pl.problems, N, s, dev, stats=True)
         ip.launch()
         torch.cuda.synchronize()
@@ -427,11 +427,13 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
         for i, p in enumerate(ps):
             goals[i, : p.goals.shape[0]] = p.goals
         starts = np.stack([p.start for p in ps])
-        res = prrtc_plan_batch(starts, goals, max_iterations=settings.max_iterations, num_new_samples=tuned[N],
+        res = prrtc_plan_batch(starts, goals, max_iterations=settings.max_iterations,
+                               num_new_samples=tuned[N]["num_new_samples"],
+                               waypoint_chunk=tuned[N]["waypoint_chunk"],
                                max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper,
                                collision_context=[p.context for p in ps], collision_checker=settings.collision_checker,
                                goal_counts=[p.goals.shape[0] for p in ps], edge_resolution=settings.edge_resolution,
-                               threads_per_explorer=settings.threads_per_explorer, return_trees=False)
+                               threads_per_explorer=tuned[N]["threads_per_explorer"], return_trees=False)
         paths = [r.path for r in res if r.solved]
         host_paths = torch.cat(paths, 0).cpu() if paths else None
         solved += sum(r.solved for r in res)
@@ -504,9 +506,10 @@ def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
         e1.synchronize()
         best = min(best, e0.elapsed_time(e1))
     torch.cuda.profiler.stop()
+    # per-test FP32 flops as issued by the kernel (prrtc_device.cuh kFlop* constants)
     S, P = 56, 960
     ns, nc, nb, nh = 32, 8, 20, 1
-    f_cfg = 7 * (90 + 63) + S * 18 + S * (ns * 10 + nc * 22 + nb * 27 + nh * 6) + P * 10
+    f_cfg = 7 * (90 + 63) + S * 18 + S * (ns * 8 + nc * 23 + nb * 27 + nh * 7) + P * 8
     ach = n * f_cfg / (best * 1e-3) / 1e12
     return {"cc_kernel": {"workload": f"tabletop scene (32 spheres, 8 capsules, 20 boxes, 1 halfspace), {n} configs, "
                                       "flat checker, full sweep", "checks_per_s": n / (best * 1e-3),

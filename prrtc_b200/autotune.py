@@ -1,9 +1,10 @@
 """Autotuner for the persistent batched planner.
 
-For one capacity bucket, times a plan of the bucket's problems with each
-candidate number of explorers per problem (samples per iteration) and keeps the
-fastest by solved plans per second; ties within 3% go to fewer explorers.
-Results are cached per (device, bucket, problem count, shape) in
+For one capacity bucket, times a plan of the bucket's problems for each
+candidate (explorers per problem = samples per iteration, threads per explorer
+CTA, waypoints per shared-memory chunk) and keeps the fastest by solved plans
+per second; a candidate must beat the incumbent by 3% to replace it.  Results
+are cached per (device, bucket, problem count, shape) in
 ``~/.cache/prrtc_b200/autotune.json``.
 """
 from __future__ import annotations
@@ -14,7 +15,10 @@ from pathlib import Path
 
 import torch
 
-CANDIDATES = (32, 64, 128, 256)
+SAMPLES = (8, 16, 32, 64, 128)
+THREADS = (64, 128)
+CHUNKS = (8, 16)
+CANDIDATES = tuple((e, t, c) for t in THREADS for c in CHUNKS for e in SAMPLES)
 CACHE = Path(os.environ.get("PRRTC_B200_CACHE", Path.home() / ".cache" / "prrtc_b200")) / "autotune.json"
 
 
@@ -32,16 +36,18 @@ def _load() -> dict:
         return {}
 
 
-def choose_samples(problems, N: int, settings, dev, candidates=CANDIDATES, use_cache: bool = True) -> int:
+def choose(problems, N: int, settings, dev, candidates=CANDIDATES, use_cache: bool = True) -> dict:
+    """Best {num_new_samples, threads_per_explorer, waypoint_chunk} for this bucket."""
     from .batch import BatchPlanner, PlanSettings
 
-    key = _key(dev, N, problems, settings)
+    key = "v2|" + _key(dev, N, problems, settings)
     cache = _load() if use_cache else {}
     if key in cache:
-        return int(cache[key])
+        return dict(cache[key])
     best, best_rate = candidates[0], -1.0
-    for E in candidates:
-        s = PlanSettings(**{**settings.__dict__, "num_new_samples": E})
+    for E, T, CW in candidates:
+        s = PlanSettings(**{**settings.__dict__, "num_new_samples": E, "threads_per_explorer": T,
+                            "waypoint_chunk": CW})
         pl = BatchPlanner(problems, N, s, dev)
         pl.launch()  # warm
         torch.cuda.synchronize(dev)
@@ -54,8 +60,9 @@ def choose_samples(problems, N: int, settings, dev, candidates=CANDIDATES, use_c
         solved = int((pl.summary_block()[:, 8] == 1).sum().item())
         rate = solved / (ms * 1e-3)
         if rate > best_rate * 1.03:
-            best, best_rate = E, rate
+            best, best_rate = (E, T, CW), rate
         del pl
+    best = {"num_new_samples": best[0], "threads_per_explorer": best[1], "waypoint_chunk": best[2]}
     if use_cache:
         cache[key] = best
         try:

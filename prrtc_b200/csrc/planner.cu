@@ -90,28 +90,38 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
         const int s1 = s.foff ? clampi(s.foff[k + 1], 0, S) : 0;
         grp[2 * k + 1] = make_float4(__int_as_float(f), __int_as_float(s0), __int_as_float(s1), 0.0f);
     }
+    // world primitives, pre-conditioned for the FMA-form tests (prrtc_device.cuh)
     float4* o_ws = reinterpret_cast<float4*>(blob + L.o_ws);
-    for (int i = tid; i < Ns; i += T) o_ws[i] = make_float4(ws[i * 4], ws[i * 4 + 1], ws[i * 4 + 2], ws[i * 4 + 3]);
+    for (int i = tid; i < Ns; i += T) {
+        const float x = ws[i * 4], y = ws[i * 4 + 1], z = ws[i * 4 + 2], r = ws[i * 4 + 3];
+        o_ws[2 * i] = make_float4(-2.0f * x, -2.0f * y, -2.0f * z, -2.0f * r);
+        o_ws[2 * i + 1] = make_float4(x, y, z, fmaf(x, x, fmaf(y, y, fmaf(z, z, -r * r))));
+    }
     float4* o_wc = reinterpret_cast<float4*>(blob + L.o_wc);
     for (int i = tid; i < Nc; i += T) {
         const float* c = &wc[i * 7];
         const float dx = c[3] - c[0], dy = c[4] - c[1], dz = c[5] - c[2];
         const float l2 = dx * dx + dy * dy + dz * dz;
-        o_wc[2 * i] = make_float4(c[0], c[1], c[2], c[6]);
-        o_wc[2 * i + 1] = make_float4(dx, dy, dz, l2 > 0.0f ? 1.0f / l2 : 0.0f);
+        const float il2 = l2 > 0.0f ? 1.0f / l2 : 0.0f;
+        const float px = dx * il2, py = dy * il2, pz = dz * il2;
+        o_wc[3 * i] = make_float4(c[0], c[1], c[2], c[6]);
+        o_wc[3 * i + 1] = make_float4(px, py, pz, -(px * c[0] + py * c[1] + pz * c[2]));
+        o_wc[3 * i + 2] = make_float4(dx, dy, dz, 0.0f);
     }
     float4* o_wb = reinterpret_cast<float4*>(blob + L.o_wb);
     for (int i = tid; i < Nb; i += T) {
         const float* c = &wbx[i * 15];
-        o_wb[4 * i] = make_float4(c[0], c[1], c[2], 0.0f);
-        o_wb[4 * i + 1] = make_float4(c[3], c[4], c[5], c[12]);
-        o_wb[4 * i + 2] = make_float4(c[6], c[7], c[8], c[13]);
-        o_wb[4 * i + 3] = make_float4(c[9], c[10], c[11], c[14]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float ax = c[3 + 3 * k], ay = c[4 + 3 * k], az = c[5 + 3 * k];
+            o_wb[4 * i + k] = make_float4(ax, ay, az, -(ax * c[0] + ay * c[1] + az * c[2]));
+        }
+        o_wb[4 * i + 3] = make_float4(c[12], c[13], c[14], 0.0f);
     }
     float4* o_wh = reinterpret_cast<float4*>(blob + L.o_wh);
     for (int i = tid; i < Nh; i += T) {
         const float* c = &wh[i * 6];
-        o_wh[i] = make_float4(c[0], c[1], c[2], c[0] * c[3] + c[1] * c[4] + c[2] * c[5]);
+        o_wh[i] = make_float4(c[0], c[1], c[2], -(c[0] * c[3] + c[1] * c[4] + c[2] * c[5]));
     }
     int2* cp = reinterpret_cast<int2*>(blob + L.o_cpair);
     for (int q = tid; q < Q; q += T) cp[q] = make_int2(s.cpairs[2 * q], s.cpairs[2 * q + 1]);
@@ -411,15 +421,21 @@ __device__ int choose_tree(int mode, int local_iter, int bid, int nblocks, int s
 }
 
 // Edge [base, base+delta] at waypoints t = (k+1)/G (prrtc_planner.cu:899-903).
+// The G waypoints are visited in nchunk interleaved passes -- pass c checks
+// waypoints c, c+nchunk, c+2*nchunk, ... -- so the first pass already samples
+// the whole edge and a colliding edge usually stops after one pass.  The
+// verdict (any waypoint in collision) does not depend on the order.
 __device__ bool cta_edge_collides(const Scene& sc, const CcBufs& B, const float* base, const float* delta, int dim,
                                   int G, int CW) {
     const int tid = threadIdx.x, T = blockDim.x;
     if (B.stats && tid == 0) atomicAdd(&B.stats[kStatEdges], 1ull);
-    for (int c0 = 0; c0 < G; c0 += CW) {
-        const int nw = min(CW, G - c0);
+    const int nchunk = (G + CW - 1) / CW;
+    for (int c = 0; c < nchunk; ++c) {
+        const int nw = (G - c + nchunk - 1) / nchunk;  // waypoints c, c+nchunk, ... below G
         for (int i = tid; i < nw * dim; i += T) {
             const int w = i / dim, d = i - w * dim;
-            const float t = __fdiv_rn((float)(c0 + w + 1), (float)G);
+            const int k = c + w * nchunk;
+            const float t = __fdiv_rn((float)(k + 1), (float)G);
             B.q[w * kDimMax + d] = __fmaf_rn(t, delta[d], base[d]);
         }
         __syncthreads();

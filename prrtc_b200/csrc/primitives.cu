@@ -152,8 +152,15 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 // Persistent over chunks of CW configurations; the scene is bulk-copied into
 // shared memory once per CTA (bounded wait; on timeout the CTA reads the scene
 // from global memory instead).
+#ifndef PRRTC_CHECK_CW
+#define PRRTC_CHECK_CW 32       // configurations per CTA pass of the batched checker
+#endif
+#ifndef PRRTC_CHECK_MINBLOCKS
+#define PRRTC_CHECK_MINBLOCKS 5 // resident CTAs per SM the register allocation must allow
+#endif
+
 template <int CW>
-__global__ void __launch_bounds__(128) check_kernel(const unsigned char* __restrict__ gblob, int blob_cap,
+__global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const unsigned char* __restrict__ gblob, int blob_cap,
                                                     const int32_t* pairs, int J, int S, int K, int Q, int dim,
                                                     const float* __restrict__ configs, int n, int full_sweep,
                                                     int32_t* verdicts) {
@@ -216,7 +223,7 @@ cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t*
                          int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
                          cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    constexpr int CW = 32;
+    constexpr int CW = PRRTC_CHECK_CW;
     const size_t cc = (size_t)cc_smem_bytes(J, S, K, Q, CW);
     size_t dyn = cc + (size_t)blob_cap;
     if (dyn + 64 > device_max_smem()) {

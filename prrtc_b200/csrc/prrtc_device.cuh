@@ -26,14 +26,17 @@ constexpr int kDimMax = 16;
 constexpr int kMaxJoints = 64;
 constexpr int kMaxLinks = 64;
 constexpr int kObsChunk = 32;    // world primitives per work item
-constexpr int kSphChunk = 8;     // fine spheres held in registers per work item
+#ifndef PRRTC_SPH_CHUNK
+#define PRRTC_SPH_CHUNK 8
+#endif
+constexpr int kSphChunk = PRRTC_SPH_CHUNK;  // fine spheres held in registers per work item
 constexpr int kPairChunk = 32;   // explicit self pairs per work item
 constexpr float kFar = 1.0e18f;  // centre of a sphere that can never collide
 
 // FP32 operations per primitive test as issued by the functions below (FFMA = 2,
 // FADD/FMUL = 1; min/max/abs and the MUFU of sin/cos/sqrt are not counted).
-constexpr int kFlopSphere = 10, kFlopCapsule = 22, kFlopBox = 27, kFlopHalfspace = 6;
-constexpr int kFlopPair = 10, kFlopPairExplicit = 11;
+constexpr int kFlopSphere = 8, kFlopCapsule = 23, kFlopBox = 27, kFlopHalfspace = 7;
+constexpr int kFlopPair = 8, kFlopPairExplicit = 11;
 constexpr int kFlopXform = 18;                  // one sphere centre
 constexpr int kFlopJointLocal = 90, kFlopJointChain = 63;
 
@@ -85,8 +88,8 @@ __host__ __device__ inline BlobLayout blob_layout(int J, int S, int K, int Q, in
     L.o_sfr = off;   off += align16(S * 4);
     L.o_grp = off;   off += K * 32;
     L.o_sch = off;   off += L.sch_cap * 16;
-    L.o_ws = off;    off += Ns * 16;
-    L.o_wc = off;    off += Nc * 32;
+    L.o_ws = off;    off += Ns * 32;
+    L.o_wc = off;    off += Nc * 48;
     L.o_wb = off;    off += Nb * 64;
     L.o_wh = off;    off += Nh * 16;
     L.o_item = off;  off += L.item_cap * 16;
@@ -102,10 +105,10 @@ struct Scene {  // typed view of a blob (shared or global memory)
     const int* sfr;
     const float4* grp;   // [K][2]: (c, r) then int4 bits (frame, s0, s1, 0)
     const int4* sch;
-    const float4* ws;
-    const float4* wc;    // [Nc][2]
-    const float4* wb;    // [Nb][4]
-    const float4* wh;
+    const float4* ws;    // [Ns][2]: (-2x,-2y,-2z,-2r), (x,y,z, x^2+y^2+z^2-r^2)
+    const float4* wc;    // [Nc][3]: (p1, r), (d/|d|^2, -p1.d/|d|^2), (d, 0)   with d = p2 - p1
+    const float4* wb;    // [Nb][4]: (a1, -a1.c), (a2, -a2.c), (a3, -a3.c), (h1, h2, h3, 0)
+    const float4* wh;    // [Nh]:    (n, -n.p)
     const int4* item;
     const int2* cpair;
     const int2* pairs;   // explicit self-pair list (global memory), for non-block items
@@ -343,98 +346,132 @@ __device__ __forceinline__ float4 xform_point(const float* F, float4 l) {
     return r;
 }
 
-// c.w carries the robot sphere radius plus the inflation margin.
-__device__ __forceinline__ bool hit_sphere(float4 c, float4 o) {
-    const float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
-    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const float t = c.w + o.w;
-    return d2 <= t * t;
+// FFMA-dense tests.  Every test yields a value that is <= 0 exactly when the
+// pair is within its threshold; a work item keeps the minimum over its spheres
+// and compares once per obstacle.
+//
+// Sphere-sphere: |c-o|^2 - (rc+ro)^2 = (|c|^2 - rc^2) + (|o|^2 - ro^2) - 2 c.o - 2 rc ro.
+// With A = |c|^2 - rc^2 per robot sphere and the obstacle stored as
+// O = (-2o, -2ro), B = |o|^2 - ro^2, the per-pair part is four FMAs:
+// g = A + c.O, and the pair collides iff g <= -B.
+__device__ __forceinline__ float sphere_A(float4 c) { return fmaf(c.x, c.x, fmaf(c.y, c.y, fmaf(c.z, c.z, -c.w * c.w))); }
+
+// Minimum of NS values as a tree (depth log2 NS instead of a serial chain).
+template <int NS>
+__device__ __forceinline__ float tree_min(float (&v)[NS]) {
+#pragma unroll
+    for (int w = 1; w < NS; w *= 2)
+#pragma unroll
+        for (int k = 0; k + w < NS; k += 2 * w) v[k] = fminf(v[k], v[k + w]);
+    return v[0];
 }
 
-__device__ __forceinline__ bool hit_capsule(float4 c, float4 p1r, float4 dl) {
-    const float wx = c.x - p1r.x, wy = c.y - p1r.y, wz = c.z - p1r.z;
-    float t = fmaf(wx, dl.x, fmaf(wy, dl.y, wz * dl.z)) * dl.w;
-    t = fminf(fmaxf(t, 0.0f), 1.0f);
-    const float ex = fmaf(-t, dl.x, wx), ey = fmaf(-t, dl.y, wy), ez = fmaf(-t, dl.z, wz);
-    const float d2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-    const float th = c.w + p1r.w;
-    return d2 <= th * th;
+template <int NS>
+__device__ __forceinline__ float min_sphere(const float4 (&c)[NS], const float (&A)[NS], float4 O) {
+    float g[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) g[k] = fmaf(c[k].x, O.x, fmaf(c[k].y, O.y, fmaf(c[k].z, O.z, fmaf(c[k].w, O.w, A[k]))));
+    return tree_min<NS>(g);
 }
 
-__device__ __forceinline__ bool hit_box(float4 c, float4 b0, float4 a1, float4 a2, float4 a3) {
-    const float px = c.x - b0.x, py = c.y - b0.y, pz = c.z - b0.z;
-    const float q1 = fmaxf(fabsf(fmaf(px, a1.x, fmaf(py, a1.y, pz * a1.z))) - a1.w, 0.0f);
-    const float q2 = fmaxf(fabsf(fmaf(px, a2.x, fmaf(py, a2.y, pz * a2.z))) - a2.w, 0.0f);
-    const float q3 = fmaxf(fabsf(fmaf(px, a3.x, fmaf(py, a3.y, pz * a3.z))) - a3.w, 0.0f);
-    const float d2 = fmaf(q1, q1, fmaf(q2, q2, q3 * q3));
-    return d2 <= c.w * c.w;
+// Capsule: t = sat(d'.c + off), e = (c - p1) - t d, g = |e|^2 - (rc + r)^2.
+template <int NS>
+__device__ __forceinline__ float min_capsule(const float4 (&c)[NS], float4 p1r, float4 dp, float4 d) {
+    float g[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const float t = __saturatef(fmaf(dp.x, c[k].x, fmaf(dp.y, c[k].y, fmaf(dp.z, c[k].z, dp.w))));
+        const float ex = fmaf(-t, d.x, c[k].x - p1r.x);
+        const float ey = fmaf(-t, d.y, c[k].y - p1r.y);
+        const float ez = fmaf(-t, d.z, c[k].z - p1r.z);
+        const float s = c[k].w + p1r.w;
+        g[k] = fmaf(ex, ex, fmaf(ey, ey, fmaf(ez, ez, -s * s)));
+    }
+    return tree_min<NS>(g);
 }
 
-__device__ __forceinline__ bool hit_halfspace(float4 c, float4 h) {
-    return fmaf(h.x, c.x, fmaf(h.y, c.y, h.z * c.z)) - h.w <= c.w;
+// Oriented box: l_k = a_k.c + off_k (box-frame coordinates), q_k = max(|l_k| - h_k, 0),
+// g = |q|^2 - r^2 (nR2 = -r^2 per sphere).  Inside the box g = -r^2 <= 0.
+template <int NS>
+__device__ __forceinline__ float min_box(const float4 (&c)[NS], const float (&nR2)[NS], float4 a1, float4 a2,
+                                         float4 a3, float4 h) {
+    float g[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const float q1 = fmaxf(fabsf(fmaf(a1.x, c[k].x, fmaf(a1.y, c[k].y, fmaf(a1.z, c[k].z, a1.w)))) - h.x, 0.0f);
+        const float q2 = fmaxf(fabsf(fmaf(a2.x, c[k].x, fmaf(a2.y, c[k].y, fmaf(a2.z, c[k].z, a2.w)))) - h.y, 0.0f);
+        const float q3 = fmaxf(fabsf(fmaf(a3.x, c[k].x, fmaf(a3.y, c[k].y, fmaf(a3.z, c[k].z, a3.w)))) - h.z, 0.0f);
+        g[k] = fmaf(q1, q1, fmaf(q2, q2, fmaf(q3, q3, nR2[k])));
+    }
+    return tree_min<NS>(g);
 }
 
-// One obstacle chunk of one type against up to 8 sphere centres held in registers.
-// Returns true on the first hit unless full_sweep; n_done = obstacles tested,
-// flop = FP32 operations of one (sphere, obstacle) test of this chunk's type.
-__device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int och, const float4 (&s)[kSphChunk],
-                                                     bool full_sweep, int& n_done, int& flop) {
+// Halfspace: g = n.c - n.p - r.
+template <int NS>
+__device__ __forceinline__ float min_halfspace(const float4 (&c)[NS], float4 hs) {
+    float g[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) g[k] = fmaf(hs.x, c[k].x, fmaf(hs.y, c[k].y, fmaf(hs.z, c[k].z, hs.w))) - c[k].w;
+    return tree_min<NS>(g);
+}
+
+__device__ __forceinline__ float4 far_sphere() { return make_float4(kFar, kFar, kFar, 0.0f); }
+
+// One obstacle chunk of one type against NS sphere centres held in registers
+// (c.w = radius + inflation; padding spheres sit at kFar).  FULL: test every
+// obstacle (no per-obstacle branch); otherwise return at the first hit.
+// n_done = obstacles tested, flop = FP32 flops of one (sphere, obstacle) test.
+template <int NS, bool FULL>
+__device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int och, const float4 (&s)[NS], int& n_done,
+                                                     int& flop) {
     const BlobHeader& h = *sc.h;
     int c = och;
-    bool hit = false;
-    n_done = 0;
     const int ns = cdiv(h.Ns, kObsChunk), nc = cdiv(h.Nc, kObsChunk), nb = cdiv(h.Nb, kObsChunk);
+    float best = INFINITY;  // minimum margin value seen (<= 0 means a hit)
+    int o0, o1;
     if (c < ns) {
         flop = kFlopSphere;
-        const int o0 = c * kObsChunk, o1 = min(h.Ns, o0 + kObsChunk);
-        for (int o = o0; o < o1; ++o) {
-            const float4 ob = sc.ws[o];
+        float A[NS];
 #pragma unroll
-            for (int k = 0; k < kSphChunk; ++k) hit |= hit_sphere(s[k], ob);
-            ++n_done;
-            if (hit && !full_sweep) return true;
+        for (int k = 0; k < NS; ++k) A[k] = sphere_A(s[k]);
+        o0 = c * kObsChunk;
+        o1 = min(h.Ns, o0 + kObsChunk);
+        for (int o = o0; o < o1; ++o) {
+            const float v = min_sphere<NS>(s, A, sc.ws[2 * o]) + sc.ws[2 * o + 1].w;
+            best = fminf(best, v);
+            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
         }
-        return hit;
-    }
-    c -= ns;
-    if (c < nc) {
+    } else if ((c -= ns) < nc) {
         flop = kFlopCapsule;
-        const int o0 = c * kObsChunk, o1 = min(h.Nc, o0 + kObsChunk);
+        o0 = c * kObsChunk;
+        o1 = min(h.Nc, o0 + kObsChunk);
         for (int o = o0; o < o1; ++o) {
-            const float4 p = sc.wc[2 * o], d = sc.wc[2 * o + 1];
-#pragma unroll
-            for (int k = 0; k < kSphChunk; ++k) hit |= hit_capsule(s[k], p, d);
-            ++n_done;
-            if (hit && !full_sweep) return true;
+            best = fminf(best, min_capsule<NS>(s, sc.wc[3 * o], sc.wc[3 * o + 1], sc.wc[3 * o + 2]));
+            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
         }
-        return hit;
-    }
-    c -= nc;
-    if (c < nb) {
+    } else if ((c -= nc) < nb) {
         flop = kFlopBox;
-        const int o0 = c * kObsChunk, o1 = min(h.Nb, o0 + kObsChunk);
-        for (int o = o0; o < o1; ++o) {
-            const float4 b0 = sc.wb[4 * o], a1 = sc.wb[4 * o + 1], a2 = sc.wb[4 * o + 2], a3 = sc.wb[4 * o + 3];
+        float nR2[NS];
 #pragma unroll
-            for (int k = 0; k < kSphChunk; ++k) hit |= hit_box(s[k], b0, a1, a2, a3);
-            ++n_done;
-            if (hit && !full_sweep) return true;
+        for (int k = 0; k < NS; ++k) nR2[k] = -s[k].w * s[k].w;
+        o0 = c * kObsChunk;
+        o1 = min(h.Nb, o0 + kObsChunk);
+        for (int o = o0; o < o1; ++o) {
+            best = fminf(best, min_box<NS>(s, nR2, sc.wb[4 * o], sc.wb[4 * o + 1], sc.wb[4 * o + 2], sc.wb[4 * o + 3]));
+            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
         }
-        return hit;
-    }
-    c -= nb;
-    {
+    } else {
+        c -= nb;
         flop = kFlopHalfspace;
-        const int o0 = c * kObsChunk, o1 = min(h.Nh, o0 + kObsChunk);
+        o0 = c * kObsChunk;
+        o1 = min(h.Nh, o0 + kObsChunk);
         for (int o = o0; o < o1; ++o) {
-            const float4 hs = sc.wh[o];
-#pragma unroll
-            for (int k = 0; k < kSphChunk; ++k) hit |= hit_halfspace(s[k], hs);
-            ++n_done;
-            if (hit && !full_sweep) return true;
+            best = fminf(best, min_halfspace<NS>(s, sc.wh[o]));
+            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
         }
     }
-    return hit;
+    n_done = o1 - o0;
+    return best <= 0.0f;
 }
 
 // ----------------------------------------------------------------------------- CTA-cooperative check
@@ -553,12 +590,10 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
                 const int och = it / (nw * K), r = it - och * (nw * K);
                 const int k = r / nw, w = r - k * nw;
                 if (B.dirty[w * KW + (k >> 5)] & (1u << (k & 31))) continue;
-                float4 s[kSphChunk];
+                float4 s[1];
                 s[0] = B.cctr[w * K + k];
-#pragma unroll
-                for (int m = 1; m < kSphChunk; ++m) s[m] = make_float4(kFar, kFar, kFar, 0.0f);
                 int nd, fl;
-                if (obstacles_vs_spheres(sc, och, s, false, nd, fl)) atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
+                if (obstacles_vs_spheres<1, false>(sc, och, s, nd, fl)) atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
                 flops += (unsigned long long)nd * fl;
             } else {
                 const int r = it - n_cw;
@@ -591,10 +626,10 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
             if (gated && ch.z >= 0 && !(B.dirty[w * KW + (ch.z >> 5)] & (1u << (ch.z & 31)))) continue;
             float4 s[kSphChunk];
 #pragma unroll
-            for (int m = 0; m < kSphChunk; ++m)
-                s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : make_float4(kFar, kFar, kFar, 0.0f);
+            for (int m = 0; m < kSphChunk; ++m) s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : far_sphere();
             int nd, fl;
-            hit = obstacles_vs_spheres(sc, och, s, full_sweep, nd, fl);
+            hit = full_sweep ? obstacles_vs_spheres<kSphChunk, true>(sc, och, s, nd, fl)
+                             : obstacles_vs_spheres<kSphChunk, false>(sc, och, s, nd, fl);
             flops += (unsigned long long)nd * fl * ch.y;
         } else {
             const int r = it - n_world;
@@ -605,18 +640,24 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
             if (gated && item.w >= 0 && !(B.gate[w * QW + (item.w >> 5)] & (1u << (item.w & 31)))) continue;
             const float4* C = &B.ctr[w * S_pad];
             if (item.y >= 0) {  // dense block: spheres [a0, a0+na) x [b0, b0+nb)
+                // self pairs use radius rho = r + inflate/2 per sphere, so the pair
+                // threshold is r_i + r_j + inflate
                 const int na = item.z >> 16, nb = item.z & 0xffff;
+                const float half = 0.5f * inflate;
                 float4 a[kSphChunk];
+                float A[kSphChunk];
 #pragma unroll
                 for (int m = 0; m < kSphChunk; ++m) {
-                    a[m] = (m < na) ? C[item.x + m] : make_float4(kFar, kFar, kFar, 0.0f);
-                    a[m].w -= inflate;
+                    a[m] = (m < na) ? C[item.x + m] : far_sphere();
+                    a[m].w -= half;
+                    A[m] = sphere_A(a[m]);
                 }
                 int bb = 0;
                 for (; bb < nb; ++bb) {
-                    const float4 b = C[item.y + bb];
-#pragma unroll
-                    for (int m = 0; m < kSphChunk; ++m) hit |= hit_sphere(a[m], b);
+                    float4 b = C[item.y + bb];
+                    b.w -= half;
+                    const float4 O = make_float4(-2.0f * b.x, -2.0f * b.y, -2.0f * b.z, -2.0f * b.w);
+                    hit |= min_sphere<kSphChunk>(a, A, O) <= -sphere_A(b);
                     if (hit && !full_sweep) { ++bb; break; }
                 }
                 flops += (unsigned long long)bb * na * kFlopPair;
@@ -634,7 +675,10 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
                 }
             }
         }
-        if (hit) atomicOr(B.hit, 1u << w);
+        // one shared-memory atomic per warp: OR the hit bits of the active lanes
+        const unsigned active = __activemask();
+        const unsigned bits = __reduce_or_sync(active, hit ? (1u << w) : 0u);
+        if (bits && (threadIdx.x & 31) == (__ffs(active) - 1)) atomicOr(B.hit, bits);
     }
     if (B.stats) {
         if (tid == 0) {

@@ -104,7 +104,8 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
         const float r = cs.w;
         float gx = 0.0f, gy = 0.0f, gz = 0.0f;
         for (int o = 0; o < h.Ns; ++o) {
-            const float4 ob = sc.ws[o];
+            const float4 o1 = sc.ws[2 * o + 1];
+            const float4 ob = make_float4(o1.x, o1.y, o1.z, -0.5f * sc.ws[2 * o].w);
             const float dx = cs.x - ob.x, dy = cs.y - ob.y, dz = cs.z - ob.z;
             const float n = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
             float sig;
@@ -113,10 +114,9 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
             gx = fmaf(k, dx, gx); gy = fmaf(k, dy, gy); gz = fmaf(k, dz, gz);
         }
         for (int o = 0; o < h.Nc; ++o) {
-            const float4 p1 = sc.wc[2 * o], dl = sc.wc[2 * o + 1];
+            const float4 p1 = sc.wc[3 * o], dp = sc.wc[3 * o + 1], dl = sc.wc[3 * o + 2];
             const float wx = cs.x - p1.x, wy = cs.y - p1.y, wz = cs.z - p1.z;
-            float t = fmaf(wx, dl.x, fmaf(wy, dl.y, wz * dl.z)) * dl.w;
-            t = fminf(fmaxf(t, 0.0f), 1.0f);
+            const float t = __saturatef(fmaf(dp.x, cs.x, fmaf(dp.y, cs.y, fmaf(dp.z, cs.z, dp.w))));
             const float ex = fmaf(-t, dl.x, wx), ey = fmaf(-t, dl.y, wy), ez = fmaf(-t, dl.z, wz);
             const float n = sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
             float sig;
@@ -125,14 +125,15 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
             gx = fmaf(k, ex, gx); gy = fmaf(k, ey, gy); gz = fmaf(k, ez, gz);
         }
         for (int o = 0; o < h.Nb; ++o) {
-            const float4 b0 = sc.wb[4 * o], ax[3] = {sc.wb[4 * o + 1], sc.wb[4 * o + 2], sc.wb[4 * o + 3]};
-            const float px = cs.x - b0.x, py = cs.y - b0.y, pz = cs.z - b0.z;
+            const float4 ax[3] = {sc.wb[4 * o], sc.wb[4 * o + 1], sc.wb[4 * o + 2]};
+            const float4 hl = sc.wb[4 * o + 3];
+            const float hh[3] = {hl.x, hl.y, hl.z};
             float l[3], qv[3], out2 = 0.0f, qmax = -INFINITY;
             int kmax = 0;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                l[k] = fmaf(px, ax[k].x, fmaf(py, ax[k].y, pz * ax[k].z));
-                qv[k] = fabsf(l[k]) - ax[k].w;
+                l[k] = fmaf(ax[k].x, cs.x, fmaf(ax[k].y, cs.y, fmaf(ax[k].z, cs.z, ax[k].w)));
+                qv[k] = fabsf(l[k]) - hh[k];
                 if (qv[k] > 0.0f) out2 = fmaf(qv[k], qv[k], out2);
                 if (qv[k] > qmax) { qmax = qv[k]; kmax = k; }
             }
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
         }
         for (int o = 0; o < h.Nh; ++o) {
             const float4 hs = sc.wh[o];
-            const float d = fmaf(hs.x, cs.x, fmaf(hs.y, cs.y, hs.z * cs.z)) - hs.w - r;
+            const float d = fmaf(hs.x, cs.x, fmaf(hs.y, cs.y, fmaf(hs.z, cs.z, hs.w))) - r;
             float sig;
             pair_term(d, a.margin, a.beta, cost, sig);
             gx = fmaf(-sig, hs.x, gx); gy = fmaf(-sig, hs.y, gy); gz = fmaf(-sig, hs.z, gz);

@@ -1,0 +1,94 @@
+"""Adjoint smoothing kernel: cost against the float64 oracle, gradient against
+central finite differences (h = 1e-3) of the oracle cost, the autograd wrapper,
+and the smoothing pass (accepted paths re-validate, rejected ones revert)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import make_problem
+
+pytestmark = pytest.mark.gpu
+
+MARGIN, BETA, WLEN = 0.02, 50.0, 1.0
+
+
+def _solved_path(orc, kind, seed):
+    pr = make_problem(kind, seed)
+    sc = orc.Scene(pr.context, pr.dim)
+    r = orc.plan(sc, pr.start, pr.goals, pr.lower, pr.upper, max_iterations=3000, num_new_samples=32,
+                 max_nodes=16384, collision_mode=3, edge_resolution=0.01)
+    assert r.solved == 1
+    return pr, sc, r.path
+
+
+def _fd_grad(sc, w, h=1e-3):
+    g = np.zeros_like(w)
+    for i in range(w.shape[0]):
+        for d in range(w.shape[1]):
+            wp, wm = w.copy(), w.copy()
+            wp[i, d] += h
+            wm[i, d] -= h
+            g[i, d] = (sc.smooth_cost(wp, MARGIN, BETA, WLEN) - sc.smooth_cost(wm, MARGIN, BETA, WLEN)) / (2 * h)
+    return g
+
+
+@pytest.mark.parametrize("kind,seed", [("tabletop", 3), ("spheres16", 1), ("uneven", 7)])
+def test_adjoint_matches_finite_differences(cuda, orc, kind, seed):
+    from prrtc_b200.smoothing import SmoothContext, resample_path
+
+    pr, sc, path = _solved_path(orc, kind, seed)
+    w = resample_path(path, 16)
+    sctx = SmoothContext(pr.context, pr.dim, MARGIN, BETA, WLEN, cuda)
+    cost, grad = sctx.cost_grad(torch.from_numpy(w)[None].to(cuda))
+    c64 = sc.smooth_cost(w.astype(np.float64), MARGIN, BETA, WLEN)
+    assert abs(cost.item() - c64) <= 1e-4 * max(1.0, abs(c64))
+    g_fd = _fd_grad(sc, w.astype(np.float64))
+    g = grad[0].cpu().numpy().astype(np.float64)
+    rel = np.linalg.norm(g - g_fd) / np.linalg.norm(g_fd)
+    assert rel < 1e-3, rel
+
+
+def test_autograd_function_and_batch(cuda, orc):
+    from prrtc_b200.smoothing import SmoothContext, resample_path, smooth_cost
+
+    pr, sc, path = _solved_path(orc, "tabletop", 4)
+    w = torch.from_numpy(np.stack([resample_path(path, 64)] * 3)).to(cuda)
+    w[1] += 0.01
+    sctx = SmoothContext(pr.context, pr.dim, MARGIN, BETA, WLEN, cuda)
+    x = w.clone().requires_grad_(True)
+    c = smooth_cost(x, sctx)
+    (c * torch.tensor([1.0, 2.0, 0.5], device=cuda)).sum().backward()
+    _, g = sctx.cost_grad(w)
+    assert torch.allclose(x.grad[0], g[0], rtol=1e-5, atol=1e-6)
+    assert torch.allclose(x.grad[1], 2.0 * g[1], rtol=1e-5, atol=1e-6)
+    assert torch.allclose(x.grad[2], 0.5 * g[2], rtol=1e-5, atol=1e-6)
+    for p in range(3):
+        c64 = sc.smooth_cost(w[p].cpu().numpy().astype(np.float64), MARGIN, BETA, WLEN)
+        assert abs(c[p].item() - c64) <= 1e-4 * max(1.0, abs(c64))
+
+
+def test_smoothing_pass_revalidates_or_reverts(cuda, orc):
+    from prrtc_b200.smoothing import smooth_paths
+
+    probs = [_solved_path(orc, "tabletop", s) for s in (10, 11, 12, 13)]
+    ctx = probs[0][0].context
+    # same world for all paths: plan each problem's start/goal in problem 0's world
+    paths = []
+    sc0 = probs[0][1]
+    for pr, _, _ in probs:
+        r = orc.plan(sc0, pr.start if sc0.in_collision(pr.start) is False else probs[0][0].start,
+                     probs[0][0].goals, pr.lower, pr.upper, max_iterations=3000, num_new_samples=32,
+                     max_nodes=16384, collision_mode=3, edge_resolution=0.01)
+        if r.solved == 1:
+            paths.append(r.path)
+    assert paths
+    out, accepted, c0, c1 = smooth_paths(paths, ctx, probs[0][0].lower, probs[0][0].upper, waypoints=64, steps=50)
+    out = out.cpu().numpy()
+    for p in range(len(paths)):
+        ok, md = sc0.validate_path(out[p], 0.01)
+        assert ok, (p, md)                       # accepted paths re-validate; rejected ones reverted
+        assert np.allclose(out[p][0], paths[p][0]) and np.allclose(out[p][-1], paths[p][-1])
+    assert bool(accepted.any())
+    assert bool((c1[accepted] <= c0[accepted] + 1e-3).all())
