@@ -18,6 +18,7 @@
  *   prrtc_b200_nearest_neighbor  <- PrrtcNearestNeighborImpl / "prrtc_nearest_neighbor"
  *                                   cuda-rrtc/CUDA/prrtc_nearest_neighbor.cu:80-141
  *   prrtc_b200_extend            <- PrrtcExtendImpl / "prrtc_extend"
+ *   prrtc_b200_iteration         <- PrrtcIterationImpl / "prrtc_iteration" (legacy)
  *                                   cuda-rrtc/CUDA/prrtc_extend.cu:76-140
  *   prrtc_b200_extract_paths     <- _trace_path + cost, cuda-rrtc/jax/prrtc.py:556-640
  *   prrtc_b200_check_configs     <- the collision checkers, prrtc_planner.cu:234-655
@@ -128,15 +129,42 @@ typedef struct {
     float collision_margin;
 } prrtc_attrs_t;
 
+/* Environment point cloud hashed into a uniform grid on the device by
+ * prrtc_b200_point_cloud_build (views into that call's workspace, which must
+ * outlive every use).  Every point is a sphere of radius r_env; a robot sphere
+ * of radius r centred at c hits point p when |c - p| <= r + r_env (the
+ * point-cloud validation of cuda-rrtc/jax/prrtc_robogpu.py:183-191, there on
+ * RT cores through an external OptiX library).  Points and sphere centres with
+ * a coordinate beyond +-1e4 m are ignored; a robot sphere whose bounding box
+ * spans more than 512 grid cells counts as a hit. */
+typedef struct {
+    const float* points;          /* [n_points,4] device, bucket-sorted (x, y, z, unused) */
+    const int32_t* bucket_start;  /* [n_buckets+1] device */
+    int32_t n_points;
+    int32_t n_buckets;            /* power of two */
+    float cell;                   /* grid cell edge (m) */
+    float r_env;
+} prrtc_point_cloud_t;
+
 /* Extensions (all-zero = defaults). */
 typedef struct {
     float edge_resolution;       /* >0: an edge gets max(granularity, ceil(len/res)) waypoints */
-    int32_t threads_per_explorer;/* CTA size of one explorer: 64, 128 or 256 (default 128) */
+    int32_t threads_per_explorer;/* threads of one explorer: 64, 128 or 256 (one explorer per CTA,
+                                    default 128), or 32 (one explorer per warp; the batched
+                                    planner then runs 4 explorers of a problem per CTA, sharing
+                                    one staged scene) */
     int32_t waypoint_chunk;      /* waypoints checked per CTA pass: 8, 16 or 32 (default 16) */
     int32_t resident_ctas;       /* batched planner grid (default: all resident CTAs) */
     uint64_t* stats;             /* optional device counters [4], accumulated: edges checked,
                                     configurations checked, FP32 flops of the collision work
                                     executed, nearest-neighbour nodes scanned */
+    const prrtc_point_cloud_t* point_cloud; /* optional environment point cloud checked by the
+                                    planner on top of the world geometry (shared by every
+                                    problem of a batch) */
+    int32_t tail_explorers;      /* batched planner: once every explorer slot has been taken,
+                                    idle CTAs join problems still running as extra explorers
+                                    (own Halton sequences); 0 = on (default), -1 = off, so
+                                    every problem keeps exactly num_new_samples explorers */
 } prrtc_tuning_t;
 
 size_t prrtc_b200_plan_workspace_size(const prrtc_inputs_t* in, const prrtc_attrs_t* attrs,
@@ -194,6 +222,19 @@ int prrtc_b200_extend(const float* tree_configs, int32_t dim, int32_t max_nodes,
                       const float* step_size, float* new_configs, int32_t* parent_indices,
                       int32_t* valid_flags, void* stream);
 
+/* Legacy single iteration ("prrtc_iteration", prrtc_iteration.cu:180-277; no
+ * collision checking): resets tree_sizes = completed = {1,1} and solved_flag =
+ * 0, then extends the smaller tree toward every sample (equal sizes: tree =
+ * sample & 1) from its nearest completed node, appending the candidates to the
+ * trees in place.  new_configs holds the float bits of each candidate.  The
+ * tree choice and slot order are those of the reference's schedule in which
+ * every sample reads the sizes before any inserts (slot 1 + sample/2). */
+int prrtc_b200_iteration(float* tree_a_configs, float* tree_b_configs, int32_t* tree_a_parents,
+                         int32_t* tree_b_parents, int32_t dim, int32_t max_nodes, const float* samples,
+                         int32_t batch, int32_t* tree_sizes, int32_t* completed, const float* step_size,
+                         int32_t* new_configs, int32_t* new_parents, int32_t* valid_flags,
+                         int32_t* solved_flag, void* stream);
+
 /* Collision verdicts of n configurations [n,dim] (1 = in collision) with the
  * checker of `collision_mode`.  full_sweep != 0 evaluates every pair with no
  * early exit (same verdicts; used to measure the kernel's FP32 throughput). */
@@ -221,6 +262,27 @@ int prrtc_b200_check_configs_noalloc(const prrtc_robot_t* robot, const prrtc_wor
                                      const float* configs, int32_t n, int32_t collision_mode,
                                      float collision_margin, int32_t full_sweep, int32_t* verdicts,
                                      void* stream);
+
+/* Point cloud [n_points,3] (device) -> hashed grid.  cell >= 1e-3 m (a cell
+ * about the largest robot sphere radius + r_env keeps queries to <= 27 cells);
+ * n_buckets a power of two <= 2^24, or 0 for the next power of two >= n_points
+ * (at least 1024). */
+size_t prrtc_b200_point_cloud_workspace_size(int32_t n_points, int32_t n_buckets);
+int prrtc_b200_point_cloud_build(const float* points, int32_t n_points, float cell, float r_env,
+                                 int32_t n_buckets, void* workspace, size_t workspace_bytes,
+                                 prrtc_point_cloud_t* cloud, void* stream);
+
+/* Edge validation (RoboGPUCollisionChecker.check_edges_collision_free, called at
+ * cuda-rrtc/jax/prrtc_robogpu.py:183-191): edges [n_edges,granularity,dim] of
+ * waypoints, free_flags [n_edges] = 1 when no waypoint collides with the world
+ * geometry, the self pairs or the point cloud (cloud may be NULL). */
+size_t prrtc_b200_check_edges_workspace_size(const prrtc_robot_t* robot, const prrtc_world_t* world,
+                                             int32_t n_edges, int32_t granularity);
+int prrtc_b200_check_edges(const prrtc_robot_t* robot, const prrtc_world_t* world,
+                           const prrtc_point_cloud_t* cloud, int32_t dim, const float* edges,
+                           int32_t n_edges, int32_t granularity, int32_t collision_mode,
+                           float collision_margin, int32_t* free_flags, void* workspace,
+                           size_t workspace_bytes, void* stream);
 
 /* Forward kinematics: frames [n,n_joints,12] (row-major R then t) in output
  * frame order. */

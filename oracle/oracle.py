@@ -59,6 +59,7 @@ class OrcScene(C.Structure):
         ("n_coarse", C.c_int), ("coarse_link", C.c_void_p), ("coarse_local", C.c_void_p),
         ("coarse_radius", C.c_void_p), ("fine_offsets", C.c_void_p),
         ("n_coarse_self", C.c_int), ("coarse_self_pairs", C.c_void_p), ("self_pair_ranges", C.c_void_p),
+        ("n_points", C.c_int), ("points", C.c_void_p), ("r_env", C.c_float),
     ]
 
 
@@ -135,6 +136,7 @@ _CTX_SPEC = {
     "coarse_sphere_link_idx": (np.int32, (-1,)), "coarse_sphere_local": (np.float32, (-1, 3)),
     "coarse_sphere_radius": (np.float32, (-1,)), "fine_link_offsets": (np.int32, (-1,)),
     "coarse_self_pairs": (np.int32, (-1, 2)), "self_pair_ranges": (np.int32, (-1, 2)),
+    "point_cloud": (np.float32, (-1, 3)),
 }
 
 
@@ -172,6 +174,8 @@ class Scene:
         s.fine_offsets = _ptr(A["fine_link_offsets"])
         s.n_coarse_self = A["coarse_self_pairs"].shape[0]
         s.coarse_self_pairs, s.self_pair_ranges = _ptr(A["coarse_self_pairs"]), _ptr(A["self_pair_ranges"])
+        s.n_points, s.points = A["point_cloud"].shape[0], _ptr(A["point_cloud"])
+        s.r_env = float(ctx.get("r_env", 0.0) or 0.0)
         self.c = s
         self.ref = C.byref(self.c)
 

@@ -277,7 +277,7 @@ static double colldist(double d, double m) {
 
 static int scene_enabled(const OrcScene* sc) {
     return sc->n_joints > 0 && sc->n_spheres > 0 &&
-           (sc->n_ws > 0 || sc->n_wc > 0 || sc->n_wb > 0 || sc->n_wh > 0 || sc->n_self > 0);
+           (sc->n_ws > 0 || sc->n_wc > 0 || sc->n_wb > 0 || sc->n_wh > 0 || sc->n_self > 0 || sc->n_points > 0);
 }
 
 static int sphere_center(const OrcScene* sc, const double* F, int s, double out[3]) {
@@ -384,11 +384,35 @@ static int check_coarse(const OrcScene* sc, const double* F) {
     return 0;
 }
 
+/* smallest |c - p| - r - r_env over the point cloud (brute force) */
+static double sphere_vs_points(const OrcScene* sc, const double* c, double r) {
+    double m = INFINITY;
+    for (int i = 0; i < sc->n_points; ++i) {
+        const float* p = &sc->points[i * 3];
+        const double dx = c[0] - p[0], dy = c[1] - p[1], dz = c[2] - p[2];
+        const double d = sqrt(dx * dx + dy * dy + dz * dz) - r - sc->r_env;
+        if (d < m) m = d;
+    }
+    return m;
+}
+
+/* Point-cloud stage: any fine sphere within r_env of a point (inflated by the
+ * margin for the differentiable checker, as the device checker does). */
+static int check_points(const OrcScene* sc, const double* F, double inflate) {
+    for (int s = 0; s < sc->n_spheres; ++s) {
+        double c[3];
+        if (!sphere_center(sc, F, s, c)) continue;
+        if (sphere_vs_points(sc, c, sc->sphere_radius[s] + inflate) <= 0) return 1;
+    }
+    return 0;
+}
+
 static int config_in_collision_d(const OrcScene* sc, const double* q, int mode, float margin) {
     if (!scene_enabled(sc)) return 0;
     if (sc->n_joints <= 0 || sc->n_joints > ORC_MAX_JOINTS) return 0;
     double F[ORC_MAX_JOINTS * 12];
     orc_fk_f64(sc, q, F);
+    if (sc->n_points > 0 && check_points(sc, F, mode == 1 ? (double)margin : 0.0)) return 1;
     const int coarse_ok = sc->n_coarse > 0 && sc->n_coarse <= ORC_MAX_LINKS;
     if (mode == 1) return check_differentiable(sc, F, margin);
     if (mode == 2 && coarse_ok) return check_coarse(sc, F);
@@ -412,8 +436,12 @@ static double min_distance_d(const OrcScene* sc, const double* q) {
     for (int s = 0; s < sc->n_spheres; ++s) {
         double c[3];
         if (!sphere_center(sc, F, s, c)) continue;
-        const double d = sphere_vs_world(sc, c, sc->sphere_radius[s], 0);
+        double d = sphere_vs_world(sc, c, sc->sphere_radius[s], 0);
         if (d < m) m = d;
+        if (sc->n_points > 0) {
+            d = sphere_vs_points(sc, c, sc->sphere_radius[s]);
+            if (d < m) m = d;
+        }
     }
     for (int p = 0; p < sc->n_self; ++p) {
         double d;

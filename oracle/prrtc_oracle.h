@@ -70,6 +70,12 @@ typedef struct {
     int n_coarse_self;
     const int* coarse_self_pairs; /* [Q,2] */
     const int* self_pair_ranges;  /* [Q,2] */
+    /* environment point cloud (the point-cloud edge validation of
+     * prrtc_robogpu.py:183-191): every point is a sphere of radius r_env,
+     * checked against every fine robot sphere by brute force */
+    int n_points;
+    const float* points;          /* [M,3] */
+    float r_env;
 } OrcScene;
 
 /* Planner attributes: the 14 FFI attributes of prrtc_planner (prrtc_planner.cu:2103-2116)

@@ -7,10 +7,12 @@ from .prrtc import (  # noqa: F401
     PRRTCResult,
     lpt_order,
     prrtc_extend,
+    prrtc_iteration,
     prrtc_nearest_neighbor,
     prrtc_plan,
     prrtc_plan_batch,
 )
+from .pointcloud import PointCloud, PointCloudChecker, prrtc_plan_robogpu  # noqa: E402,F401
 
 __all__ = [
     "PRRTCResult",
@@ -18,5 +20,9 @@ __all__ = [
     "prrtc_plan_batch",
     "prrtc_nearest_neighbor",
     "prrtc_extend",
+    "prrtc_iteration",
     "lpt_order",
+    "PointCloud",
+    "PointCloudChecker",
+    "prrtc_plan_robogpu",
 ]

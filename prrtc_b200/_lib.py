@@ -64,10 +64,16 @@ class Attrs(C.Structure):
     ]
 
 
+class PointCloud(C.Structure):
+    _fields_ = [
+        ("points", P), ("bucket_start", P), ("n_points", I32), ("n_buckets", I32), ("cell", F32), ("r_env", F32),
+    ]
+
+
 class Tuning(C.Structure):
     _fields_ = [
         ("edge_resolution", F32), ("threads_per_explorer", I32), ("waypoint_chunk", I32),
-        ("resident_ctas", I32), ("stats", P),
+        ("resident_ctas", I32), ("stats", P), ("point_cloud", P), ("tail_explorers", I32),
     ]
 
 
@@ -90,6 +96,9 @@ EXPORTS = (
     "prrtc_b200_nearest_neighbor_workspace_size", "prrtc_b200_nearest_neighbor",
     "prrtc_b200_extend",
     "prrtc_b200_check_configs_workspace_size", "prrtc_b200_check_configs",
+    "prrtc_b200_iteration",
+    "prrtc_b200_point_cloud_workspace_size", "prrtc_b200_point_cloud_build",
+    "prrtc_b200_check_edges_workspace_size", "prrtc_b200_check_edges",
     "prrtc_b200_fk", "prrtc_b200_halton", "prrtc_b200_extract_paths",
     "prrtc_b200_smooth_workspace_size", "prrtc_b200_smooth_cost_grad",
     "prrtc_b200_fp32_probe",
@@ -106,6 +115,11 @@ _SIGS = {
     "prrtc_b200_extend": (C.c_int, [P, I32, I32, P, P, I32, P, P, P, P, P]),
     "prrtc_b200_check_configs_workspace_size": (C.c_size_t, [P, P]),
     "prrtc_b200_check_configs": (C.c_int, [P, P, I32, P, I32, I32, F32, I32, P, P, C.c_size_t, P]),
+    "prrtc_b200_iteration": (C.c_int, [P, P, P, P, I32, I32, P, I32, P, P, P, P, P, P, P, P]),
+    "prrtc_b200_point_cloud_workspace_size": (C.c_size_t, [I32, I32]),
+    "prrtc_b200_point_cloud_build": (C.c_int, [P, I32, F32, F32, I32, P, C.c_size_t, P, P]),
+    "prrtc_b200_check_edges_workspace_size": (C.c_size_t, [P, P, I32, I32]),
+    "prrtc_b200_check_edges": (C.c_int, [P, P, P, I32, P, I32, I32, I32, F32, P, P, C.c_size_t, P]),
     "prrtc_b200_fk": (C.c_int, [P, I32, P, I32, P, P]),
     "prrtc_b200_halton": (C.c_int, [I32, I32, I32, P, P, P, P]),
     "prrtc_b200_extract_paths": (C.c_int, [I32, I32, I32, P, P, P, P, P, P, I32, P, P, P, P]),

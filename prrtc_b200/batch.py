@@ -38,6 +38,7 @@ class PlanSettings:
     threads_per_explorer: int = 128
     waypoint_chunk: int = 16
     resident_ctas: int = 0
+    tail_explorers: bool = True
 
 
 class BatchPlanner:
@@ -95,7 +96,8 @@ class BatchPlanner:
         self.attrs = _attrs(s.max_iterations, s.step_size, s.num_new_samples, s.balance_mode, s.tree_ratio,
                             s.dynamic_domain, s.dd_alpha, s.dd_radius, s.dd_min_radius, dim, self.N, s.granularity,
                             _resolve_collision_mode(s.collision_checker), s.collision_margin)
-        self.tun = _tuning(s.edge_resolution, s.threads_per_explorer, s.waypoint_chunk, s.resident_ctas)
+        self.tun = _tuning(s.edge_resolution, s.threads_per_explorer, s.waypoint_chunk, s.resident_ctas,
+                           s.tail_explorers)
         self.stats = torch.zeros(4, dtype=torch.int64, device=self.dev) if stats else None
         if self.stats is not None:
             self.tun.stats = self.stats.data_ptr()
@@ -127,7 +129,8 @@ class BatchPlanner:
         self.res.extract(sp)
 
     def capture(self) -> None:
-        """Capture launch() as a CUDA graph (warm up once first)."""
+        """Capture launch() as a CUDA graph (warm up once first).  Replays go to
+        the caller's current stream."""
         s = torch.cuda.Stream(device=self.dev)
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):

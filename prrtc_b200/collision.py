@@ -18,7 +18,9 @@ from .prrtc import _resolve_collision_mode
 
 
 class CollisionChecker:
-    """A collision context resident on the GPU, reusable across calls."""
+    """A collision context resident on the GPU, reusable across calls.  A
+    context with a ``point_cloud`` entry [M,3] (and ``r_env``) is checked
+    against the cloud too."""
 
     def __init__(self, collision_context: dict, dim: int, collision_checker: str = "binary",
                  collision_margin: float = 0.02, device=None):
@@ -32,6 +34,9 @@ class CollisionChecker:
         self._world = self.ctx.world()
         self.ws = workspace(self.lib.prrtc_b200_check_configs_workspace_size(C.byref(self._robot),
                                                                            C.byref(self._world)), self.device)
+        from .pointcloud import cloud_from_context
+
+        self.cloud = cloud_from_context(collision_context, self.device)
 
     def check(self, configs, full_sweep: bool = False, out: torch.Tensor | None = None,
               stream: torch.cuda.Stream | None = None) -> torch.Tensor:
@@ -40,6 +45,16 @@ class CollisionChecker:
         n = int(cf.shape[0])
         if out is None:
             out = torch.empty((n,), dtype=torch.int32, device=self.device)
+        if self.cloud is not None:  # one-waypoint edges through the edge checker, which sees the cloud
+            free = torch.empty((n,), dtype=torch.int32, device=self.device)
+            ws = workspace(self.lib.prrtc_b200_check_edges_workspace_size(C.byref(self._robot), C.byref(self._world),
+                                                                         n, 1), self.device)
+            _lib.check(self.lib.prrtc_b200_check_edges(C.byref(self._robot), C.byref(self._world), self.cloud.ref(),
+                                                       self.dim, ptr(cf), n, 1, self.mode, self.margin, ptr(free),
+                                                       ws.data_ptr(), ws.numel(), stream_handle(stream)),
+                       "prrtc_b200_check_edges")
+            torch.sub(1, free, out=out)
+            return out
         _lib.check(self.lib.prrtc_b200_check_configs(C.byref(self._robot), C.byref(self._world), self.dim, ptr(cf),
                                                      n, self.mode, self.margin, 1 if full_sweep else 0, ptr(out),
                                                      self.ws.data_ptr(), self.ws.numel(), stream_handle(stream)),

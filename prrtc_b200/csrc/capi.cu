@@ -84,17 +84,37 @@ struct Tuned {
     float edge_res;
     int threads, cw, resident;
     unsigned long long* stats;
+    const prrtc_point_cloud_t* cloud;
+    int tail_join;
 };
 
+static PcView pc_view(const prrtc_point_cloud_t* c) {
+    if (!c || c->n_points <= 0 || !c->points || !c->bucket_start) return PcView{nullptr, nullptr, 0, 0, 0.0f, 0.0f};
+    return PcView{reinterpret_cast<const float4*>(c->points), c->bucket_start, c->n_points, c->n_buckets - 1,
+                  1.0f / c->cell, c->r_env};
+}
+
+// A cloud descriptor is usable when its bucket count is a power of two and its
+// cell and radius are sane (NULL or empty = no cloud).
+static bool cloud_ok(const prrtc_point_cloud_t* c) {
+    if (!c || c->n_points == 0) return true;
+    const int H = c->n_buckets;
+    return c->n_points > 0 && c->points && c->bucket_start && H > 0 && (H & (H - 1)) == 0 && H <= (1 << 24) &&
+           c->cell >= 1e-3f && c->r_env >= 0.0f && aligned(c->points, 16);
+}
+
 static Tuned tuned(const prrtc_tuning_t* t) {
-    Tuned o{0.0f, 128, 16, 0, nullptr};
+    Tuned o{0.0f, 128, 16, 0, nullptr, nullptr, 1};
     if (t) {
         if (t->edge_resolution > 0.0f) o.edge_res = t->edge_resolution;
-        if (t->threads_per_explorer == 64 || t->threads_per_explorer == 128 || t->threads_per_explorer == 256)
+        if (t->threads_per_explorer == 32 || t->threads_per_explorer == 64 || t->threads_per_explorer == 128 ||
+            t->threads_per_explorer == 256)
             o.threads = t->threads_per_explorer;
         if (t->waypoint_chunk == 8 || t->waypoint_chunk == 16 || t->waypoint_chunk == 32) o.cw = t->waypoint_chunk;
         if (t->resident_ctas > 0) o.resident = t->resident_ctas;
         o.stats = reinterpret_cast<unsigned long long*>(t->stats);
+        o.cloud = t->point_cloud;
+        o.tail_join = t->tail_explorers < 0 ? 0 : 1;
     }
     return o;
 }
@@ -112,6 +132,9 @@ static void fill_launch(PlanLaunch& L, const prrtc_outputs_t* out, const prrtc_a
     L.dd_alpha = a->dd_alpha; L.dd_radius = a->dd_radius; L.dd_min_radius = a->dd_min_radius;
     L.edge_res = tu.edge_res; L.threads = tu.threads; L.cw = tu.cw; L.resident = tu.resident;
     L.stats = tu.stats;
+    L.warp_explorers = tu.threads == 32;
+    L.pc = pc_view(tu.cloud);
+    L.tail_join = tu.tail_join;
 }
 
 static bool outputs_ok(const prrtc_outputs_t* o) {
@@ -153,12 +176,14 @@ int prrtc_b200_plan(const prrtc_inputs_t* in, const prrtc_outputs_t* out, const 
         return PRRTC_B200_EARG;
     if (in->num_goals < 1 || in->num_goals > a->max_nodes) return PRRTC_B200_EARG;
     if ((rc = check_robot(in->robot))) return rc;
-    const PackSrc s = make_pack(in->robot, in->world, a->dim, a->collision_mode, a->collision_margin);
+    const Tuned tu = tuned(tuning);
+    if (!cloud_ok(tu.cloud)) return PRRTC_B200_EARG;
+    PackSrc s = make_pack(in->robot, in->world, a->dim, a->collision_mode, a->collision_margin);
+    s.has_cloud = pc_view(tu.cloud).n > 0;
     const size_t stride = blob_stride(s);
     if (!ws || !aligned(ws, 256) || ws_bytes < plan_workspace_bytes(1, a->max_nodes, stride))
         return PRRTC_B200_EWORKSPACE;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const Tuned tu = tuned(tuning);
     PlanLaunch L;
     memset(&L, 0, sizeof(L));
     L.B = 1;
@@ -209,12 +234,14 @@ int prrtc_b200_plan_batch(const prrtc_batch_inputs_t* in, const prrtc_outputs_t*
         return PRRTC_B200_EARG;
     if (in->num_goals < 1 || in->num_goals > a->max_nodes) return PRRTC_B200_EARG;
     if ((rc = check_robot(in->robot))) return rc;
-    const PackSrc s = make_batch_pack(in, a->dim, a->collision_mode, a->collision_margin);
+    const Tuned tu = tuned(tuning);
+    if (!cloud_ok(tu.cloud)) return PRRTC_B200_EARG;
+    PackSrc s = make_batch_pack(in, a->dim, a->collision_mode, a->collision_margin);
+    s.has_cloud = pc_view(tu.cloud).n > 0;
     const size_t stride = blob_stride(s);
     if (!ws || !aligned(ws, 256) || ws_bytes < plan_workspace_bytes(in->batch, a->max_nodes, stride))
         return PRRTC_B200_EWORKSPACE;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const Tuned tu = tuned(tuning);
     PlanLaunch L;
     memset(&L, 0, sizeof(L));
     L.B = in->batch;
@@ -264,6 +291,20 @@ int prrtc_b200_extend(const float* tree, int32_t dim, int32_t max_nodes, const i
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 
+int prrtc_b200_iteration(float* ta, float* tb, int32_t* pa, int32_t* pb, int32_t dim, int32_t max_nodes,
+                         const float* samples, int32_t batch, int32_t* sizes, int32_t* completed, const float* step,
+                         int32_t* new_cfg, int32_t* new_par, int32_t* valid, int32_t* solved, void* stream) {
+    if (batch == 0) return PRRTC_B200_OK;
+    if (!ta || !tb || !pa || !pb || !samples || !sizes || !completed || !step || !new_cfg || !new_par || !valid ||
+        !solved || batch < 0 || max_nodes < 1)
+        return PRRTC_B200_EARG;
+    if (dim < 1 || dim > PRRTC_B200_DIM_MAX) return PRRTC_B200_EUNSUPPORTED;
+    if ((long long)batch * 32 > INT32_MAX) return PRRTC_B200_EUNSUPPORTED;
+    cudaError_t e = launch_iteration(ta, tb, pa, pb, dim, max_nodes, samples, batch, sizes, completed, step, new_cfg,
+                                     new_par, valid, solved, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
 size_t prrtc_b200_check_configs_workspace_size(const prrtc_robot_t* robot, const prrtc_world_t* world) {
     if (!robot || !world) return 0;
     return blob_stride(make_pack(*robot, *world, 1, 0, 0.0f));
@@ -286,6 +327,74 @@ int prrtc_b200_check_configs(const prrtc_robot_t* robot, const prrtc_world_t* wo
     if (e != cudaSuccess) return cuda_fail(e);
     e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, configs, n, full_sweep, verdicts,
                      st);
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
+static int pc_buckets(int32_t n_points, int32_t n_buckets) {
+    if (n_buckets > 0) return n_buckets;
+    int H = 1024;
+    while (H < n_points && H < (1 << 24)) H <<= 1;
+    return H;
+}
+
+size_t prrtc_b200_point_cloud_workspace_size(int32_t n_points, int32_t n_buckets) {
+    if (n_points < 0) return 0;
+    const int H = pc_buckets(n_points, n_buckets);
+    return pc_workspace_bytes(n_points, H);
+}
+
+int prrtc_b200_point_cloud_build(const float* points, int32_t n_points, float cell, float r_env, int32_t n_buckets,
+                                 void* ws, size_t ws_bytes, prrtc_point_cloud_t* cloud, void* stream) {
+    if (!cloud || n_points < 0 || (n_points > 0 && !points) || n_buckets < 0) return PRRTC_B200_EARG;
+    if (!(cell >= 1e-3f) || !(r_env >= 0.0f) || !(r_env < 1e3f)) return PRRTC_B200_EARG;
+    const int H = pc_buckets(n_points, n_buckets);
+    if ((H & (H - 1)) != 0 || H > (1 << 24)) return PRRTC_B200_EUNSUPPORTED;
+    if (!ws || !aligned(ws, 256) || ws_bytes < pc_workspace_bytes(n_points, H)) return PRRTC_B200_EWORKSPACE;
+    PcView v;
+    cudaError_t e = launch_pc_build(points, n_points, cell, r_env, H, ws, &v, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e);
+    cloud->points = reinterpret_cast<const float*>(v.pts);
+    cloud->bucket_start = v.start;
+    cloud->n_points = n_points;
+    cloud->n_buckets = H;
+    cloud->cell = cell;
+    cloud->r_env = r_env;
+    return PRRTC_B200_OK;
+}
+
+size_t prrtc_b200_check_edges_workspace_size(const prrtc_robot_t* robot, const prrtc_world_t* world,
+                                             int32_t n_edges, int32_t granularity) {
+    if (!robot || !world || n_edges < 0 || granularity < 0) return 0;
+    const size_t blob = blob_stride(make_pack(*robot, *world, 1, 0, 0.0f));
+    return blob + ((((size_t)n_edges * granularity * sizeof(int32_t)) + 255) & ~(size_t)255);
+}
+
+int prrtc_b200_check_edges(const prrtc_robot_t* robot, const prrtc_world_t* world, const prrtc_point_cloud_t* cloud,
+                           int32_t dim, const float* edges, int32_t n_edges, int32_t G, int32_t mode, float margin,
+                           int32_t* free_flags, void* ws, size_t ws_bytes, void* stream) {
+    if (n_edges == 0) return PRRTC_B200_OK;
+    if (!robot || !world || !edges || !free_flags || n_edges < 0 || G < 1 || mode < 0 || mode > 3)
+        return PRRTC_B200_EARG;
+    if (dim < 1 || dim > PRRTC_B200_DIM_MAX) return PRRTC_B200_EUNSUPPORTED;
+    if ((long long)n_edges * G > INT32_MAX) return PRRTC_B200_EUNSUPPORTED;
+    if (!cloud_ok(cloud)) return PRRTC_B200_EARG;
+    int rc = check_robot(*robot);
+    if (rc) return rc;
+    PackSrc s = make_pack(*robot, *world, dim, mode, margin);
+    const PcView pc = pc_view(cloud);
+    s.has_cloud = pc.n > 0;
+    const size_t stride = blob_stride(s);
+    if (!ws || !aligned(ws, 256) || ws_bytes < prrtc_b200_check_edges_workspace_size(robot, world, n_edges, G))
+        return PRRTC_B200_EWORKSPACE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char* blob = static_cast<unsigned char*>(ws);
+    int32_t* verdicts = reinterpret_cast<int32_t*>(blob + stride);
+    cudaError_t e = launch_pack(s, 1, blob, stride, st);
+    if (e != cudaSuccess) return cuda_fail(e);
+    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, edges, n_edges * G, 0, verdicts,
+                     st, &pc);
+    if (e != cudaSuccess) return cuda_fail(e);
+    e = launch_edge_reduce(verdicts, n_edges, G, free_flags, st);
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 

@@ -8,6 +8,21 @@
 
 namespace prrtc {
 
+// Environment point cloud in a hashed uniform grid: points sorted by bucket,
+// bucket b holding points [start[b], start[b+1]).  Cell (ix,iy,iz) =
+// floor(p / cell) hashes to a bucket with the spatial hash of Teschner et al.
+// (2003), three large primes XORed; cells that share a bucket only cost extra
+// distance tests.  Every point is a sphere of radius r_env.
+struct PcView {
+    const float4* pts;  // [n] (x, y, z, unused)
+    const int* start;   // [mask + 2]
+    int n;              // 0 = no cloud
+    int mask;           // buckets - 1 (power of two)
+    float inv_cell;
+    float r_env;
+};
+
+
 // Sources of the packed scene of every problem in a launch.  Robot tables are
 // shared; world tables are either shared (count pointers null, n = max) or
 // batched [B, max, feat] with per-problem device counts.
@@ -25,6 +40,7 @@ struct PackSrc {
     int mode;
     float margin;
     int dim;
+    int has_cloud;  // an environment point cloud is checked too (enables collision checking)
 };
 
 // Capacity in bytes of one problem's blob (multiple of 256).
@@ -45,7 +61,7 @@ struct PlanLaunch {
     unsigned char* blobs; size_t blob_stride; int blob_cap;
     float* radii;                      // [B][2][N]
     unsigned long long* tstamp;        // [B][2]
-    int32_t* queue;                    // [2]: head, error
+    int32_t* queue;                    // [3]: head, error, tail-join ticket
     // shape
     int B, E, N, dim, J, S, K, Q;
     // attributes
@@ -54,7 +70,10 @@ struct PlanLaunch {
     // tuning
     int threads, cw, resident;
     int persistent;
+    int warp_explorers;                // persistent form with 32 threads: one explorer per warp (4 per CTA)
+    int tail_join;                     // persistent form: idle CTAs join running problems as extra explorers
     unsigned long long* stats;         // optional device counters (kStat*)
+    PcView pc;                         // environment point cloud shared by every problem (pc.n = 0: none)
 };
 
 size_t plan_workspace_bytes(int B, int N, size_t blob_stride);
@@ -70,9 +89,20 @@ cudaError_t launch_nearest(const float* tree, int dim, int N, const int32_t* tre
 cudaError_t launch_extend(const float* tree, int dim, int N, const int32_t* nearest, const float* samples,
                           int batch, const float* step, float* out, int32_t* parents, int32_t* valid,
                           cudaStream_t st);
+cudaError_t launch_iteration(float* ta, float* tb, int32_t* pa, int32_t* pb, int dim, int N, const float* samples,
+                             int batch, int32_t* sizes, int32_t* completed, const float* step, int32_t* new_cfg,
+                             int32_t* new_par, int32_t* valid, int32_t* solved, cudaStream_t st);
 cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t* pairs, int J, int S, int K,
                          int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
-                         cudaStream_t st);
+                         cudaStream_t st, const PcView* pc = nullptr);
+
+// pointcloud.cu
+size_t pc_workspace_bytes(int n_points, int n_buckets);
+// Hash n_points points [n,3] into n_buckets (power of two) buckets of cells of
+// edge `cell`; fills `view` with pointers into the workspace.
+cudaError_t launch_pc_build(const float* points, int n_points, float cell, float r_env, int n_buckets, void* ws,
+                            PcView* view, cudaStream_t st);
+cudaError_t launch_edge_reduce(const int32_t* verdicts, int n_edges, int G, int32_t* free_flags, cudaStream_t st);
 struct FkTables {
     const float* twists; const float* ptf; const int32_t* parent; const int32_t* act;
     const float* mmul; const float* moff; const int32_t* mact; const int32_t* topo_inv; int J;

@@ -65,7 +65,8 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
     const BlobLayout L = blob_layout(J, S, K, Q, s.sp_max, s.ws_max, s.wc_max, s.wb_max, s.wh_max);
 
     // reference enable rules (prrtc_planner.cu:505-506, 1156-1157, 1173, 741-743)
-    const bool enabled = J > 0 && J <= kMaxJoints && S > 0 && (Ns > 0 || Nc > 0 || Nb > 0 || Nh > 0 || P > 0);
+    const bool enabled =
+        J > 0 && J <= kMaxJoints && S > 0 && (Ns > 0 || Nc > 0 || Nb > 0 || Nh > 0 || P > 0 || s.has_cloud);
     const bool coarse_ok = K > 0 && K <= kMaxLinks && s.foff != nullptr;
     bool gated = enabled && coarse_ok && (s.mode == 2 || (s.mode == 3 && J <= 16));
 
@@ -284,14 +285,15 @@ __device__ bool stage_blob(unsigned char* dst, const unsigned char* src, int byt
 
 // ============================================================================ nearest neighbour
 
-// CTA-wide argmin of the squared distance from q (shared memory) over nodes
+// Group-wide argmin of the squared distance from q (shared memory) over nodes
 // [0, n) of the SoA tree (row stride N).  dsq = d0*d0, then fma(dd, dd, dsq) in
 // dimension order -- bit-identical to the reference's `dsq += diff*diff`
 // (prrtc_planner.cu:845-849) under nvcc's default contraction.  Result:
 // red_d[0], red_i[0] (INT_MAX when no valid node).
-__device__ void cta_nearest(const float* __restrict__ tree, int N, int dim, int n, const float* q, float* red_d,
-                            int* red_i) {
-    const int tid = threadIdx.x, T = blockDim.x;
+template <class G>
+__device__ void group_nearest(const G& grp, const float* __restrict__ tree, int N, int dim, int n, const float* q,
+                              float* red_d, int* red_i) {
+    const int tid = grp.rank(), T = grp.size();
     float best = INFINITY;
     int bi = INT_MAX;
     float qr[kDimMax];
@@ -339,21 +341,26 @@ __device__ void cta_nearest(const float* __restrict__ tree, int N, int dim, int 
         const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
         if (od < best || (od == best && oi < bi)) { best = od; bi = oi; }
     }
-    const int warp = tid >> 5, lane = tid & 31, nwarp = (T + 31) >> 5;
-    if (lane == 0) { red_d[warp] = best; red_i[warp] = bi; }
-    __syncthreads();
-    if (warp == 0) {
-        best = lane < nwarp ? red_d[lane] : INFINITY;
-        bi = lane < nwarp ? red_i[lane] : INT_MAX;
+    if constexpr (G::kWarp) {
+        if (tid == 0) { red_d[0] = best; red_i[0] = bi; }
+        grp.sync();
+    } else {
+        const int warp = tid >> 5, lane = tid & 31, nwarp = (T + 31) >> 5;
+        if (lane == 0) { red_d[warp] = best; red_i[warp] = bi; }
+        __syncthreads();
+        if (warp == 0) {
+            best = lane < nwarp ? red_d[lane] : INFINITY;
+            bi = lane < nwarp ? red_i[lane] : INT_MAX;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const float od = __shfl_xor_sync(0xffffffffu, best, off);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-            if (od < best || (od == best && oi < bi)) { best = od; bi = oi; }
+            for (int off = 16; off > 0; off >>= 1) {
+                const float od = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (od < best || (od == best && oi < bi)) { best = od; bi = oi; }
+            }
+            if (lane == 0) { red_d[0] = best; red_i[0] = bi; }
         }
-        if (lane == 0) { red_d[0] = best; red_i[0] = bi; }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 // ============================================================================ explorer
@@ -395,8 +402,25 @@ struct ExplorerSmem {
     int order[16];
     int halton[kDimMax];
     int stop, t, n_t, n_o, nn, skip, new_idx, n_ext, ext_parent, ext_idx, G1, G2, vamp, cnn, abort_;
-    int slot, problem;
+    int slot, problem, join_e;
 };
+
+// Tail join: once every explorer slot has been taken, a CTA that runs out of
+// work picks a problem that is still running -- round-robin over the problems
+// from a global ticket -- and runs an extra explorer on it (explorer index
+// E + ticket: its own Halton sequence).  The hardest problems of a batch thus
+// end with every idle CTA exploring them instead of E explorers and an idle
+// GPU.  Returns the problem, or -1 when none is running.
+__device__ int tail_join_pick(const PlanLaunch& L, int* e_out) {
+    const int k = atomicAdd(&L.queue[2], 1);
+    *e_out = L.E + k;
+    for (int i = 0; i < L.B; ++i) {
+        const int pi = (int)(((long long)k + i) % L.B);
+        const int bb = L.order ? L.order[pi] : pi;
+        if (ld_volatile(&L.solved[bb]) == 0) return bb;
+    }
+    return -1;
+}
 
 // Tree side (prrtc_planner.cu:790-824); nblocks = explorers of this problem.
 __device__ int choose_tree(int mode, int local_iter, int bid, int nblocks, int size_a, int size_b, float thr,
@@ -425,9 +449,10 @@ __device__ int choose_tree(int mode, int local_iter, int bid, int nblocks, int s
 // waypoints c, c+nchunk, c+2*nchunk, ... -- so the first pass already samples
 // the whole edge and a colliding edge usually stops after one pass.  The
 // verdict (any waypoint in collision) does not depend on the order.
-__device__ bool cta_edge_collides(const Scene& sc, const CcBufs& B, const float* base, const float* delta, int dim,
-                                  int G, int CW) {
-    const int tid = threadIdx.x, T = blockDim.x;
+template <class Grp>
+__device__ bool group_edge_collides(const Grp& grp, const Scene& sc, const CcBufs& B, const float* base,
+                                    const float* delta, int dim, int G, int CW) {
+    const int tid = grp.rank(), T = grp.size();
     if (B.stats && tid == 0) atomicAdd(&B.stats[kStatEdges], 1ull);
     const int nchunk = (G + CW - 1) / CW;
     for (int c = 0; c < nchunk; ++c) {
@@ -438,8 +463,8 @@ __device__ bool cta_edge_collides(const Scene& sc, const CcBufs& B, const float*
             const float t = __fdiv_rn((float)(k + 1), (float)G);
             B.q[w * kDimMax + d] = __fmaf_rn(t, delta[d], base[d]);
         }
-        __syncthreads();
-        if (cc_chunk(sc, B, nw, true, false) != 0u) return true;
+        grp.sync();
+        if (cc_chunk(grp, sc, B, nw, true, false) != 0u) return true;
     }
     return false;
 }
@@ -449,17 +474,18 @@ __device__ __forceinline__ void stamp_end(const Prob& P) {
 }
 
 // One explorer (problem P, index e of E) until the problem terminates or the
-// explorer exits.  All threads of the CTA call it.
-__device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc, const CcBufs& B,
+// explorer exits.  All threads of the group call it.
+template <class Grp>
+__device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P, const Scene& sc, const CcBufs& B,
                              ExplorerSmem& X, int e) {
-    const int tid = threadIdx.x;
+    const int tid = grp.rank();
     const int dim = L.dim, N = L.N;
     if (tid == 0) {
         prime_order(e, X.order);
         for (int d = 0; d < kDimMax; ++d) X.halton[d] = 1;
         X.vamp = 0;
     }
-    __syncthreads();
+    grp.sync();
     int local_iter = 0;
     while (true) {
         ++local_iter;
@@ -473,16 +499,16 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
             if (!stop) {
                 halton_sample(X.order, X.halton, dim, L.lo, L.hi, X.sample);
                 const int sa = ld_volatile(&P.sizes[0]), sb = ld_volatile(&P.sizes[1]);
-                const int t = choose_tree(L.balance_mode, local_iter, e, L.E, sa, sb, L.tree_ratio, X.vamp);
+                const int t = choose_tree(L.balance_mode, local_iter, e % L.E, L.E, sa, sb, L.tree_ratio, X.vamp);
                 X.t = t;
                 X.n_t = min(t == 0 ? sa : sb, N);
             }
             X.stop = stop;
         }
-        __syncthreads();
+        grp.sync();
         if (X.stop) break;
         const int t = X.t, o = 1 - t;
-        cta_nearest(P.tree[t], N, dim, X.n_t, X.sample, X.red_d, X.red_i);
+        group_nearest(grp, P.tree[t], N, dim, X.n_t, X.sample, X.red_d, X.red_i);
         if (tid == 0) {
             if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_t);
             const int nn = X.red_i[0];
@@ -504,9 +530,9 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
             X.nn = nn;
             X.skip = skip;
         }
-        __syncthreads();
+        grp.sync();
         if (X.skip) continue;
-        if (cta_edge_collides(sc, B, X.base, X.delta, dim, X.G1, L.cw)) {
+        if (group_edge_collides(grp, sc, B, X.base, X.delta, dim, X.G1, L.cw)) {
             if (tid == 0 && L.dd) radius_shrink(P.radii[t], X.nn, L.dd_alpha, L.dd_radius, L.dd_min_radius);
             continue;
         }
@@ -522,16 +548,16 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
                 X.new_idx = idx;
             }
         }
-        __syncthreads();
+        grp.sync();
         if (X.new_idx < 0) break;
         if (tid < dim) __stcg(&P.tree[t][(size_t)tid * N + X.new_idx], X.cand[tid]);
         if (tid == 0) {
             atomicAdd(&P.completed[t], 1);
             X.n_o = min(ld_volatile(&P.sizes[o]), N);
         }
-        __syncthreads();
+        grp.sync();
         // connect (prrtc_planner.cu:949-1043)
-        cta_nearest(P.tree[o], N, dim, X.n_o, X.cand, X.red_d, X.red_i);
+        group_nearest(grp, P.tree[o], N, dim, X.n_o, X.cand, X.red_d, X.red_i);
         if (tid == 0) {
             if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_o);
             const int cnn = X.red_i[0];
@@ -554,12 +580,12 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
             X.ext_parent = X.new_idx;
             X.abort_ = 0;
         }
-        __syncthreads();
+        grp.sync();
         bool failed = X.n_ext < 0;
         const int n_ext = X.n_ext;
         for (int ext = 0; ext < n_ext && !failed; ++ext) {
             if (X.abort_) { failed = true; break; }
-            if (cta_edge_collides(sc, B, X.curr, X.vec, dim, X.G2, L.cw)) { failed = true; break; }
+            if (group_edge_collides(grp, sc, B, X.curr, X.vec, dim, X.G2, L.cw)) { failed = true; break; }
             if (tid == 0) {
                 const int eidx = atomicAdd(&P.sizes[t], 1);
                 if (eidx >= N) {
@@ -572,14 +598,14 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
                     X.ext_idx = eidx;
                 }
             }
-            __syncthreads();
+            grp.sync();
             if (X.ext_idx < 0) { failed = true; break; }
             if (tid < dim) __stcg(&P.tree[t][(size_t)tid * N + X.ext_idx], X.curr[tid]);
             if (tid == 0) {
                 atomicAdd(&P.completed[t], 1);
                 X.abort_ = ld_volatile(P.solved) != 0;
             }
-            __syncthreads();
+            grp.sync();
         }
         if (!failed) {  // connection found (prrtc_planner.cu:1045-1062)
             if (tid == 0) {
@@ -594,7 +620,7 @@ __device__ void run_explorer(const PlanLaunch& L, const Prob& P, const Scene& sc
             break;
         }
     }
-    __syncthreads();
+    grp.sync();
 }
 
 // Plain form: grid = E explorers of problem blockIdx.y.  Persistent form: CTAs
@@ -627,13 +653,20 @@ __global__ void __launch_bounds__(256) explore_kernel(PlanLaunch L) {
                     slot = atomicAdd(&L.queue[0], 1);
                 }
                 X.slot = slot;
+                X.problem = -1;
+                if (slot >= total && L.tail_join) X.problem = tail_join_pick(L, &X.join_e);
             }
             __syncthreads();
             const int slot = X.slot;
-            if (slot >= total) break;
-            const int pi = slot / L.E;
-            b = L.order ? L.order[pi] : pi;
-            e = slot - pi * L.E;
+            if (slot < total) {
+                const int pi = slot / L.E;
+                b = L.order ? L.order[pi] : pi;
+                e = slot - pi * L.E;
+            } else {
+                if (X.problem < 0) break;
+                b = X.problem;
+                e = X.join_e;
+            }
         } else {
             if (iter > 0) break;
             b = blockIdx.y;
@@ -649,11 +682,86 @@ __global__ void __launch_bounds__(256) explore_kernel(PlanLaunch L) {
                 sc = scene_view(gblob);
             }
             sc.pairs = reinterpret_cast<const int2*>(L.pairs) + (size_t)b * L.pairs_stride;
+            sc.pc = L.pc;
             cur = b;
         }
         const Prob P = prob_ptrs(L, b);
         if (L.persistent && tid == 0) atomicCAS(&P.ts[0], 0ull, globaltimer());
-        run_explorer(L, P, sc, B, X, e);
+        run_explorer(CtaGroup{}, L, P, sc, B, X, e);
+    }
+}
+
+// Persistent batched form with one explorer per warp: a CTA pops a group of
+// kWarpsPerCta explorer slots of one problem, stages that problem's scene once,
+// and each warp runs one explorer with warp-level synchronisation only.
+constexpr int kWarpsPerCta = 4;
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32) explore_warps_kernel(PlanLaunch L) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ ExplorerSmem Xs[kWarpsPerCta];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int s_group;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const bool staged = L.blob_cap > 0;
+    unsigned char* blob_sm = dsm;
+    const int ccb = cc_smem_bytes(L.J, L.S, L.K, L.Q, L.cw);
+    CcBufs B = cc_bufs(dsm + (staged ? L.blob_cap : 0) + warp * ccb, L.J, L.S, L.K, L.Q, L.cw);
+    B.stats = L.stats;
+    ExplorerSmem& X = Xs[warp];
+    if (tid == 0) mbar_init(&mbar);
+    __syncthreads();
+    uint32_t phase = 0;
+    int cur = -1;
+    Scene sc;
+    const int gpp = (L.E + kWarpsPerCta - 1) / kWarpsPerCta;  // slot groups per problem
+    const int total = L.B * gpp;
+    __shared__ int s_join_b, s_join_e;
+    while (true) {
+        if (tid == 0) {
+            int g = atomicAdd(&L.queue[0], 1);
+            while (g < total) {  // skip problems that already terminated
+                const int pi = g / gpp;
+                const int bb = L.order ? L.order[pi] : pi;
+                if (ld_volatile(&L.solved[bb]) == 0) break;
+                g = atomicAdd(&L.queue[0], 1);
+            }
+            s_group = g;
+            s_join_b = -1;
+            if (g >= total && L.tail_join) {
+                int e0;
+                s_join_b = tail_join_pick(L, &e0);
+                s_join_e = L.E + (e0 - L.E) * kWarpsPerCta;  // four distinct extra explorers
+            }
+        }
+        __syncthreads();
+        const int g = s_group;
+        int b, e;
+        if (g < total) {
+            const int pi = g / gpp;
+            b = L.order ? L.order[pi] : pi;
+            e = (g - pi * gpp) * kWarpsPerCta + warp;
+        } else {
+            if (s_join_b < 0) break;
+            b = s_join_b;
+            e = s_join_e + warp;
+        }
+        const unsigned char* gblob = L.blobs + (size_t)b * L.blob_stride;
+        if (b != cur) {
+            if (staged) {
+                const int bytes = reinterpret_cast<const BlobHeader*>(gblob)->used_bytes;
+                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1])) break;
+                sc = scene_view(blob_sm);
+            } else {
+                sc = scene_view(gblob);
+            }
+            sc.pairs = reinterpret_cast<const int2*>(L.pairs) + (size_t)b * L.pairs_stride;
+            sc.pc = L.pc;
+            cur = b;
+        }
+        const Prob P = prob_ptrs(L, b);
+        if (tid == 0) atomicCAS(&P.ts[0], 0ull, globaltimer());
+        if (e < L.E || g >= total) run_explorer(WarpGroup{}, L, P, sc, B, X, e);
+        __syncthreads();  // every warp done with this problem before the next pop
     }
 }
 
@@ -684,7 +792,7 @@ __global__ void init_kernel(PlanLaunch L, int stamp_start) {
         P.ts[0] = stamp_start ? globaltimer() : 0ull;
         P.ts[1] = 0ull;
     }
-    if (b == 0 && tid == 0) { L.queue[0] = 0; L.queue[1] = 0; }
+    if (b == 0 && tid == 0) { L.queue[0] = 0; L.queue[1] = 0; L.queue[2] = 0; }
 }
 
 __global__ void finalize_kernel(PlanLaunch L) {
@@ -740,27 +848,32 @@ cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
     init_kernel<<<L.B, 128, 0, st>>>(L, L.persistent ? 0 : 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
-    const size_t cc = (size_t)cc_smem_bytes(L.J, L.S, L.K, L.Q, L.cw);
+    const size_t ccb = (size_t)cc_smem_bytes(L.J, L.S, L.K, L.Q, L.cw);
     const size_t max_smem = device_max_smem();
-    const size_t static_smem = sizeof(ExplorerSmem) + 64;
+    // one explorer per warp needs four checker buffers; fall back to one
+    // explorer per (single-warp) CTA when they do not fit
+    const bool warps = L.persistent && L.warp_explorers &&
+                       (ccb + sizeof(ExplorerSmem)) * kWarpsPerCta + 64 <= max_smem;
+    const size_t cc = ccb * (warps ? kWarpsPerCta : 1);
+    const size_t static_smem = sizeof(ExplorerSmem) * (warps ? kWarpsPerCta : 1) + 64;
     size_t dyn = cc + (size_t)L.blob_cap;
     if (dyn + static_smem > max_smem) {  // scene too large to stage: read it from global memory
         L.blob_cap = 0;
         dyn = cc;
     }
-    if ((e = cudaFuncSetAttribute(explore_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) !=
-        cudaSuccess)
+    auto kern = warps ? explore_warps_kernel : explore_kernel;
+    const int threads = warps ? kWarpsPerCta * 32 : L.threads;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) != cudaSuccess)
         return e;
     if (L.persistent) {
         int per_sm = 0;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, explore_kernel, L.threads, dyn)) !=
-            cudaSuccess)
-            return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, dyn)) != cudaSuccess) return e;
         per_sm = std::max(per_sm, 1);
         long long grid = (long long)per_sm * device_sm_count();
         if (L.resident > 0) grid = std::min<long long>(grid, L.resident);
-        grid = std::min<long long>(grid, (long long)L.B * L.E);
-        explore_kernel<<<(unsigned)std::max<long long>(grid, 1), L.threads, dyn, st>>>(L);
+        const long long work = warps ? (long long)L.B * ((L.E + kWarpsPerCta - 1) / kWarpsPerCta) : (long long)L.B * L.E;
+        grid = std::min<long long>(grid, work);
+        kern<<<(unsigned)std::max<long long>(grid, 1), threads, dyn, st>>>(L);
     } else {
         explore_kernel<<<dim3(L.E, L.B), L.threads, dyn, st>>>(L);
     }

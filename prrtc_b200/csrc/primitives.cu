@@ -81,6 +81,79 @@ __global__ void __launch_bounds__(256) nn_kernel(const float* __restrict__ tree,
     }
 }
 
+// Query-tiled form for batches: CTA (s, t) scans its slice once for QT queries
+// of tile t.  Each thread keeps one 4-node column of every dimension in
+// registers and evaluates all QT queries (held in shared memory) against it, so
+// the tree is read once per QT queries instead of once per query.  Arithmetic
+// per (node, query) is the same sub/mul/fma sequence as nn_kernel.
+template <int QT>
+__global__ void __launch_bounds__(256) nn_tiled_kernel(const float* __restrict__ tree, int dim, int N,
+                                                       const int32_t* tree_size, const float* __restrict__ q,
+                                                       int batch, int slice, unsigned long long* keys) {
+    __shared__ __align__(16) float qs[QT][kDimMax];
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int q0 = blockIdx.y * QT;
+    for (int i = tid; i < QT * kDimMax; i += T) {
+        const int qq = i / kDimMax, d = i - qq * kDimMax;
+        qs[qq][d] = (q0 + qq < batch && d < dim) ? q[(size_t)(q0 + qq) * dim + d] : 0.0f;
+    }
+    __syncthreads();
+    int n = tree_size ? tree_size[0] : N;
+    n = max(1, min(n, N));
+    const int lo = blockIdx.x * slice;
+    const int hi = min(n, lo + slice);
+    float best[QT];
+    int bi[QT];
+#pragma unroll
+    for (int k = 0; k < QT; ++k) { best[k] = INFINITY; bi[k] = INT_MAX; }
+    const float4* t4 = reinterpret_cast<const float4*>(tree);
+    const size_t row4 = (size_t)(N >> 2);
+    const int g0 = lo >> 2, g1 = (hi + 3) >> 2;
+    for (int g = g0 + tid; g < g1; g += T) {
+        float4 v[kDimMax];
+#pragma unroll
+        for (int d = 0; d < kDimMax; ++d)
+            if (d < dim) v[d] = __ldg(t4 + d * row4 + g);
+        const int i0 = g << 2;
+#pragma unroll
+        for (int k = 0; k < QT; ++k) {
+            float dx = __fsub_rn(v[0].x, qs[k][0]), dy = __fsub_rn(v[0].y, qs[k][0]), dz = __fsub_rn(v[0].z, qs[k][0]),
+                  dw = __fsub_rn(v[0].w, qs[k][0]);
+            float ax = __fmul_rn(dx, dx), ay = __fmul_rn(dy, dy), az = __fmul_rn(dz, dz), aw = __fmul_rn(dw, dw);
+#pragma unroll
+            for (int d = 1; d < kDimMax; ++d) {
+                if (d < dim) {
+                    const float qd = qs[k][d];
+                    dx = __fsub_rn(v[d].x, qd); dy = __fsub_rn(v[d].y, qd);
+                    dz = __fsub_rn(v[d].z, qd); dw = __fsub_rn(v[d].w, qd);
+                    ax = __fmaf_rn(dx, dx, ax); ay = __fmaf_rn(dy, dy, ay);
+                    az = __fmaf_rn(dz, dz, az); aw = __fmaf_rn(dw, dw, aw);
+                }
+            }
+            if (ax < best[k] && i0 < hi) { best[k] = ax; bi[k] = i0; }
+            if (ay < best[k] && i0 + 1 < hi) { best[k] = ay; bi[k] = i0 + 1; }
+            if (az < best[k] && i0 + 2 < hi) { best[k] = az; bi[k] = i0 + 2; }
+            if (aw < best[k] && i0 + 3 < hi) { best[k] = aw; bi[k] = i0 + 3; }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < QT; ++k) {
+        float bk = best[k];
+        int ik = bi[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float od = __shfl_xor_sync(0xffffffffu, bk, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, ik, off);
+            if (od < bk || (od == bk && oi < ik)) { bk = od; ik = oi; }
+        }
+        if ((tid & 31) == 0 && ik != INT_MAX && q0 + k < batch) {
+            const unsigned long long key =
+                ((unsigned long long)__float_as_uint(bk) << 32) | (unsigned long long)(unsigned)ik;
+            atomicMin(&keys[q0 + k], key);
+        }
+    }
+}
+
 __global__ void nn_decode_kernel(const unsigned long long* keys, int batch, int32_t* idx, float* dist) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= batch) return;
@@ -101,11 +174,17 @@ cudaError_t launch_nearest(const float* tree, int dim, int N, const int32_t* tre
     if (e != cudaSuccess) return e;
     // enough CTAs to cover every SM several times; slices are multiples of 1024 nodes
     const int sms = device_sm_count();
-    int splits = std::max(1, (4 * sms + batch - 1) / batch);
+    constexpr int kQT = 8;
+    const bool tiled = batch >= 4 && (N & 3) == 0 && (reinterpret_cast<uintptr_t>(tree) & 15) == 0;
+    const int tiles = tiled ? (batch + kQT - 1) / kQT : batch;
+    int splits = std::max(1, (4 * sms + tiles - 1) / tiles);
     int slice = (N + splits - 1) / splits;
     slice = std::max(1024, (slice + 1023) & ~1023);
     splits = (N + slice - 1) / slice;
-    nn_kernel<<<dim3(splits, batch), 256, 0, st>>>(tree, dim, N, tree_size, q, batch, slice, keys);
+    if (tiled)
+        nn_tiled_kernel<kQT><<<dim3(splits, tiles), 256, 0, st>>>(tree, dim, N, tree_size, q, batch, slice, keys);
+    else
+        nn_kernel<<<dim3(splits, batch), 256, 0, st>>>(tree, dim, N, tree_size, q, batch, slice, keys);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     nn_decode_kernel<<<(batch + 255) / 256, 256, 0, st>>>(keys, batch, idx, dist);
     return cudaGetLastError();
@@ -143,6 +222,68 @@ cudaError_t launch_extend(const float* tree, int dim, int N, const int32_t* near
     return cudaGetLastError();
 }
 
+// ============================================================================ legacy iteration
+
+// prrtc_iteration.cu:21-167 (the "prrtc_iteration" target): every call first
+// resets the state to one node per tree, then each sample extends the smaller
+// tree (equal sizes: tree = sample & 1) from its nearest node among the
+// `completed` ones and appends the step-limited candidate.  The reference reads
+// the live sizes and appends with atomics, so its tree choice and slot order
+// depend on scheduling; here every sample sees the sizes after the reset and
+// the samples of a tree take its slots in sample order -- the schedule in which
+// every block reads before any block inserts.  One warp per sample.
+__global__ void iteration_kernel(float* ta, float* tb, int32_t* pa, int32_t* pb, int dim, int N,
+                                 const float* __restrict__ samples, int batch, int32_t* sizes, int32_t* completed,
+                                 const float* step_ptr, int32_t* new_cfg, int32_t* new_par, int32_t* valid,
+                                 int32_t* solved) {
+    // state after the reset (prrtc_iteration.cu:28-45): sizes = completed = {1, 1}
+    const int n0 = (batch + 1) >> 1, n1 = batch >> 1;  // samples per tree under the tie rule
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int room = max(0, N - 1);
+        sizes[0] = completed[0] = 1 + min(n0, room);
+        sizes[1] = completed[1] = 1 + min(n1, room);
+        solved[0] = 0;
+    }
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (b >= batch) return;
+    const int t = b & 1;
+    float* tree = t == 0 ? ta : tb;
+    int32_t* par = t == 0 ? pa : pb;
+    const float* q = samples + (size_t)b * dim;
+    // nearest among the completed nodes [0, 1): the root
+    const int nn = 0;
+    float dsq = 0.0f;
+    for (int d = 0; d < dim; ++d) {
+        const float df = __fsub_rn(tree[(size_t)d * N + nn], q[d]);
+        dsq = d == 0 ? __fmul_rn(df, df) : __fmaf_rn(df, df, dsq);
+    }
+    const float nd = __fsqrt_rn(dsq);
+    const float step = step_ptr[0];
+    const float scale = nd > 1e-8f ? fminf(1.0f, __fdiv_rn(step, nd)) : 1.0f;
+    const int idx = 1 + (b >> 1);  // this sample's slot in tree t
+    const bool ok = idx < N;
+    for (int d = lane; d < dim; d += 32) {
+        const float nv = tree[(size_t)d * N + nn];
+        const float c = __fmaf_rn(__fsub_rn(q[d], nv), scale, nv);
+        new_cfg[(size_t)b * dim + d] = __float_as_int(c);
+        if (ok) tree[(size_t)d * N + idx] = c;
+    }
+    if (lane == 0) {
+        new_par[b] = nn;
+        valid[b] = ok ? 1 : 0;
+        if (ok) par[idx] = nn;
+    }
+}
+
+cudaError_t launch_iteration(float* ta, float* tb, int32_t* pa, int32_t* pb, int dim, int N, const float* samples,
+                             int batch, int32_t* sizes, int32_t* completed, const float* step, int32_t* new_cfg,
+                             int32_t* new_par, int32_t* valid, int32_t* solved, cudaStream_t st) {
+    const int blocks = std::max(1, (batch * 32 + 127) / 128);
+    iteration_kernel<<<blocks, 128, 0, st>>>(ta, tb, pa, pb, dim, N, samples, batch, sizes, completed, step, new_cfg,
+                                             new_par, valid, solved);
+    return cudaGetLastError();
+}
+
 // ============================================================================ batched collision check
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -163,7 +304,7 @@ template <int CW>
 __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const unsigned char* __restrict__ gblob, int blob_cap,
                                                     const int32_t* pairs, int J, int S, int K, int Q, int dim,
                                                     const float* __restrict__ configs, int n, int full_sweep,
-                                                    int32_t* verdicts) {
+                                                    int32_t* verdicts, PcView pc) {
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ __align__(8) uint64_t mbar;
     const int tid = threadIdx.x;
@@ -207,6 +348,7 @@ __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const
         sc = scene_view(gblob);
     }
     sc.pairs = reinterpret_cast<const int2*>(pairs);
+    sc.pc = pc;
     for (int c0 = blockIdx.x * CW; c0 < n; c0 += gridDim.x * CW) {
         const int nw = min(CW, n - c0);
         for (int i = tid; i < nw * dim; i += blockDim.x) {
@@ -214,15 +356,16 @@ __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const
             B.q[w * kDimMax + d] = configs[(size_t)(c0 + w) * dim + d];
         }
         __syncthreads();
-        const uint32_t hit = cc_chunk(sc, B, nw, false, full_sweep != 0);
+        const uint32_t hit = cc_chunk(CtaGroup{}, sc, B, nw, false, full_sweep != 0);
         for (int w = tid; w < nw; w += blockDim.x) verdicts[c0 + w] = (hit >> w) & 1u;
     }
 }
 
 cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t* pairs, int J, int S, int K,
                          int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
-                         cudaStream_t st) {
+                         cudaStream_t st, const PcView* pc) {
     if (n <= 0) return cudaSuccess;
+    const PcView cloud = pc ? *pc : PcView{nullptr, nullptr, 0, 0, 0.0f, 0.0f};
     constexpr int CW = PRRTC_CHECK_CW;
     const size_t cc = (size_t)cc_smem_bytes(J, S, K, Q, CW);
     size_t dyn = cc + (size_t)blob_cap;
@@ -238,7 +381,7 @@ cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t*
     const long long chunks = (n + CW - 1) / CW;
     const long long grid = std::min<long long>(chunks, (long long)std::max(per_sm, 1) * device_sm_count());
     check_kernel<CW><<<(unsigned)grid, 128, dyn, st>>>(blob, blob_cap, pairs, J, S, K, Q, dim, configs, n,
-                                                        full_sweep, verdicts);
+                                                        full_sweep, verdicts, cloud);
     return cudaGetLastError();
 }
 

@@ -20,6 +20,8 @@
 #include <float.h>
 #include <stdint.h>
 
+#include "kernels.h"
+
 namespace prrtc {
 
 constexpr int kDimMax = 16;
@@ -98,6 +100,14 @@ __host__ __device__ inline BlobLayout blob_layout(int J, int S, int K, int Q, in
     return L;
 }
 
+constexpr float kPcExtent = 1.0e4f;  // points and sphere centres beyond +-10 km are ignored
+constexpr int kPcMaxCells = 512;     // a sphere spanning more grid cells is reported as a hit
+constexpr int kFlopPoint = 8;        // 3 FADD + FMUL + 2 FFMA per point test
+
+__device__ __forceinline__ unsigned pc_hash(int x, int y, int z, int mask) {
+    return ((unsigned)x * 73856093u ^ (unsigned)y * 19349663u ^ (unsigned)z * 83492791u) & (unsigned)mask;
+}
+
 struct Scene {  // typed view of a blob (shared or global memory)
     const BlobHeader* h;
     const JointRec* joints;
@@ -112,6 +122,7 @@ struct Scene {  // typed view of a blob (shared or global memory)
     const int4* item;
     const int2* cpair;
     const int2* pairs;   // explicit self-pair list (global memory), for non-block items
+    PcView pc;           // environment point cloud (global memory), pc.n == 0 when absent
 };
 
 __device__ __forceinline__ Scene scene_view(const unsigned char* b) {
@@ -129,7 +140,42 @@ __device__ __forceinline__ Scene scene_view(const unsigned char* b) {
     s.item = reinterpret_cast<const int4*>(b + s.h->o_item);
     s.cpair = reinterpret_cast<const int2*>(b + s.h->o_cpair);
     s.pairs = nullptr;
+    s.pc = PcView{nullptr, nullptr, 0, 0, 0.0f, 0.0f};
     return s;
+}
+
+// Sphere c (c.w = radius + inflation) against the point cloud: any point p with
+// |c - p| <= c.w + r_env.  Visits every grid cell the sphere's bounding box
+// touches; a box of more than kPcMaxCells cells is conservatively a hit.  With
+// |c| < kPcExtent, 0 <= R < 1e3 and a cell of at least 1 mm every cell index
+// stays below 2^31 in magnitude.
+__device__ inline bool pc_sphere_hits(const PcView& pc, float4 c, bool full_sweep, unsigned long long& flops) {
+    if (!(fabsf(c.x) < kPcExtent && fabsf(c.y) < kPcExtent && fabsf(c.z) < kPcExtent)) return false;
+    const float R = c.w + pc.r_env;
+    if (!(R >= 0.0f)) return false;  // negative or NaN radius: touches nothing
+    if (!(R < 1.0e3f)) return true;  // a sphere of 1 km or more is conservatively a hit
+    const float R2 = R * R;
+    const int x0 = (int)floorf((c.x - R) * pc.inv_cell), x1 = (int)floorf((c.x + R) * pc.inv_cell);
+    const int y0 = (int)floorf((c.y - R) * pc.inv_cell), y1 = (int)floorf((c.y + R) * pc.inv_cell);
+    const int z0 = (int)floorf((c.z - R) * pc.inv_cell), z1 = (int)floorf((c.z + R) * pc.inv_cell);
+    const long long cells = ((long long)x1 - x0 + 1) * ((long long)y1 - y0 + 1) * ((long long)z1 - z0 + 1);
+    if (cells > kPcMaxCells) return true;
+    bool hit = false;
+    for (int z = z0; z <= z1; ++z)
+        for (int y = y0; y <= y1; ++y)
+            for (int x = x0; x <= x1; ++x) {
+                const unsigned b = pc_hash(x, y, z, pc.mask);
+                const int p1 = __ldg(&pc.start[b + 1]);
+                int p = __ldg(&pc.start[b]);
+                flops += (unsigned long long)(p1 - p) * kFlopPoint;
+                for (; p < p1; ++p) {
+                    const float4 q = __ldg(&pc.pts[p]);
+                    const float dx = c.x - q.x, dy = c.y - q.y, dz = c.z - q.z;
+                    hit |= fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= R2;
+                    if (hit && !full_sweep) return true;
+                }
+            }
+    return hit;
 }
 
 // ----------------------------------------------------------------------------- small helpers
@@ -417,62 +463,105 @@ __device__ __forceinline__ float min_halfspace(const float4 (&c)[NS], float4 hs)
 
 __device__ __forceinline__ float4 far_sphere() { return make_float4(kFar, kFar, kFar, 0.0f); }
 
-// One obstacle chunk of one type against NS sphere centres held in registers
-// (c.w = radius + inflation; padding spheres sit at kFar).  FULL: test every
-// obstacle (no per-obstacle branch); otherwise return at the first hit.
-// n_done = obstacles tested, flop = FP32 flops of one (sphere, obstacle) test.
+// World obstacles form one list in type order (spheres, capsules, boxes,
+// halfspaces).  Work items take contiguous ranges of that list of roughly equal
+// cost; the weights are the issue slots of one sphere test of each type.
+constexpr int kCostSphere = 5, kCostCapsule = 15, kCostBox = 19, kCostHalfspace = 5;
+
+__device__ __forceinline__ int world_cost(const BlobHeader& h) {
+    return kCostSphere * h.Ns + kCostCapsule * h.Nc + kCostBox * h.Nb + kCostHalfspace * h.Nh;
+}
+
+// First obstacle (combined index) whose cost offset is >= x.
+__device__ __forceinline__ int world_index_at(const BlobHeader& h, int x) {
+    int base = 0, cbase = 0;
+    const int n[4] = {h.Ns, h.Nc, h.Nb, h.Nh};
+    const int w[4] = {kCostSphere, kCostCapsule, kCostBox, kCostHalfspace};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int span = n[t] * w[t];
+        if (x <= cbase + span) return base + (x - cbase + w[t] - 1) / w[t];
+        base += n[t];
+        cbase += span;
+    }
+    return base;
+}
+
+// Obstacles [j0, j1) of the combined list against NS sphere centres held in
+// registers (c.w = radius + inflation; padding spheres sit at kFar).  FULL:
+// test every obstacle without a per-obstacle branch; otherwise return at the
+// first hit.  flops accumulates the FP32 flops of the tests executed (NS_real
+// real spheres per test).
 template <int NS, bool FULL>
-__device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int och, const float4 (&s)[NS], int& n_done,
-                                                     int& flop) {
+__device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int j0, int j1, const float4 (&s)[NS],
+                                                     int ns_real, unsigned long long& flops) {
     const BlobHeader& h = *sc.h;
-    int c = och;
-    const int ns = cdiv(h.Ns, kObsChunk), nc = cdiv(h.Nc, kObsChunk), nb = cdiv(h.Nb, kObsChunk);
     float best = INFINITY;  // minimum margin value seen (<= 0 means a hit)
-    int o0, o1;
-    if (c < ns) {
-        flop = kFlopSphere;
+    int lo = max(j0, 0), hi = min(j1, h.Ns);
+    if (lo < hi) {
         float A[NS];
 #pragma unroll
         for (int k = 0; k < NS; ++k) A[k] = sphere_A(s[k]);
-        o0 = c * kObsChunk;
-        o1 = min(h.Ns, o0 + kObsChunk);
-        for (int o = o0; o < o1; ++o) {
-            const float v = min_sphere<NS>(s, A, sc.ws[2 * o]) + sc.ws[2 * o + 1].w;
-            best = fminf(best, v);
-            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
+        for (int o = lo; o < hi; ++o) {
+            best = fminf(best, min_sphere<NS>(s, A, sc.ws[2 * o]) + sc.ws[2 * o + 1].w);
+            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopSphere; return true; }
         }
-    } else if ((c -= ns) < nc) {
-        flop = kFlopCapsule;
-        o0 = c * kObsChunk;
-        o1 = min(h.Nc, o0 + kObsChunk);
-        for (int o = o0; o < o1; ++o) {
+        flops += (unsigned long long)(hi - lo) * ns_real * kFlopSphere;
+    }
+    int base = h.Ns;
+    lo = max(j0, base) - base;
+    hi = min(j1, base + h.Nc) - base;
+    if (lo < hi) {
+        for (int o = lo; o < hi; ++o) {
             best = fminf(best, min_capsule<NS>(s, sc.wc[3 * o], sc.wc[3 * o + 1], sc.wc[3 * o + 2]));
-            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
+            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopCapsule; return true; }
         }
-    } else if ((c -= nc) < nb) {
-        flop = kFlopBox;
+        flops += (unsigned long long)(hi - lo) * ns_real * kFlopCapsule;
+    }
+    base += h.Nc;
+    lo = max(j0, base) - base;
+    hi = min(j1, base + h.Nb) - base;
+    if (lo < hi) {
         float nR2[NS];
 #pragma unroll
         for (int k = 0; k < NS; ++k) nR2[k] = -s[k].w * s[k].w;
-        o0 = c * kObsChunk;
-        o1 = min(h.Nb, o0 + kObsChunk);
-        for (int o = o0; o < o1; ++o) {
+        for (int o = lo; o < hi; ++o) {
             best = fminf(best, min_box<NS>(s, nR2, sc.wb[4 * o], sc.wb[4 * o + 1], sc.wb[4 * o + 2], sc.wb[4 * o + 3]));
-            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
+            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopBox; return true; }
         }
-    } else {
-        c -= nb;
-        flop = kFlopHalfspace;
-        o0 = c * kObsChunk;
-        o1 = min(h.Nh, o0 + kObsChunk);
-        for (int o = o0; o < o1; ++o) {
-            best = fminf(best, min_halfspace<NS>(s, sc.wh[o]));
-            if (!FULL && best <= 0.0f) { n_done = o - o0 + 1; return true; }
-        }
+        flops += (unsigned long long)(hi - lo) * ns_real * kFlopBox;
     }
-    n_done = o1 - o0;
+    base += h.Nb;
+    lo = max(j0, base) - base;
+    hi = min(j1, base + h.Nh) - base;
+    if (lo < hi) {
+        for (int o = lo; o < hi; ++o) {
+            best = fminf(best, min_halfspace<NS>(s, sc.wh[o]));
+            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopHalfspace; return true; }
+        }
+        flops += (unsigned long long)(hi - lo) * ns_real * kFlopHalfspace;
+    }
     return best <= 0.0f;
 }
+
+// ----------------------------------------------------------------------------- thread groups
+
+// The checker, the nearest-neighbour scan and the explorer loop run either on a
+// whole CTA (one explorer per CTA) or on one warp (one explorer per warp, four
+// per CTA); the group type supplies the rank, size and barrier.
+struct CtaGroup {
+    static constexpr bool kWarp = false;
+    __device__ __forceinline__ int rank() const { return threadIdx.x; }
+    __device__ __forceinline__ int size() const { return blockDim.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+struct WarpGroup {
+    static constexpr bool kWarp = true;
+    __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+    __device__ __forceinline__ int size() const { return 32; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
 
 // ----------------------------------------------------------------------------- CTA-cooperative check
 
@@ -519,13 +608,15 @@ __device__ inline CcBufs cc_bufs(unsigned char* base, int J, int S, int K, int Q
 }
 
 // Collision check of nw (<= CW <= 32) configurations already in B.q.  Every
-// thread of the CTA must call it.  edge_mode: stop all work at the first hit
+// thread of the group must call it.  edge_mode: stop all work at the first hit
 // (the whole edge is rejected).  Otherwise each configuration stops at its own
 // first hit, or never with full_sweep.  Returns the hit bit mask (bit w =
 // configuration w in collision).
-__device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bool edge_mode, bool full_sweep) {
+template <class G>
+__device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B, int nw, bool edge_mode,
+                                    bool full_sweep) {
     const BlobHeader& h = *sc.h;
-    const int tid = threadIdx.x, T = blockDim.x;
+    const int tid = g.rank(), T = g.size();
     const int J = h.J, S = h.S, S_pad = h.S_pad, K = h.K, Q = h.Q;
     const bool gated = h.gated != 0;
     const float inflate = __int_as_float(h.inflate_bits);
@@ -533,7 +624,7 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
     volatile uint32_t* vhit = B.hit;
 
     if (!h.enabled) {
-        __syncthreads();
+        g.sync();
         return 0u;
     }
     if (tid == 0) *vhit = 0u;
@@ -547,7 +638,7 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
         const JointRec& jr = sc.joints[j];
         joint_local(jr, joint_value(jr, &B.q[w * kDimMax]), &B.pose[(w * J + j) * 12]);
     }
-    __syncthreads();
+    g.sync();
     // B: chain composition in topological order, one waypoint per thread
     for (int w = tid; w < nw; w += T) {
         float* P = &B.pose[w * J * 12];
@@ -556,7 +647,7 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
             if (p >= 0 && p < j) compose(&P[p * 12], &P[j * 12], &P[j * 12]);
         }
     }
-    __syncthreads();
+    g.sync();
     // C: sphere centres (fine, and coarse when gated)
     for (int it = tid; it < nw * S; it += T) {
         const int w = it / S, s = it - w * S;
@@ -580,21 +671,27 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
             B.cctr[w * K + k] = c;
         }
     }
-    __syncthreads();
+    g.sync();
     unsigned long long flops = 0;
+    // World work is split into n_parts ranges of the combined obstacle list with
+    // about equal cost, enough parts for roughly two world items per thread.
+    const int n_obs = h.Ns + h.Nc + h.Nb + h.Nh;
+    const int ctot = world_cost(h);
+    const int n_parts = n_obs == 0 ? 0 : max(1, min(cdiv(2 * T, max(1, nw * h.n_sch)), cdiv(n_obs, 4)));
     // D: coarse pre-pass -> dirty groups and touching coarse self pairs
     if (gated) {
-        const int n_cw = nw * K * h.n_och;
+        const int n_cw = nw * K * n_parts;
         for (int it = tid; it < n_cw + nw * Q; it += T) {
             if (it < n_cw) {
-                const int och = it / (nw * K), r = it - och * (nw * K);
+                const int part = it / (nw * K), r = it - part * (nw * K);
                 const int k = r / nw, w = r - k * nw;
                 if (B.dirty[w * KW + (k >> 5)] & (1u << (k & 31))) continue;
                 float4 s[1];
                 s[0] = B.cctr[w * K + k];
-                int nd, fl;
-                if (obstacles_vs_spheres<1, false>(sc, och, s, nd, fl)) atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
-                flops += (unsigned long long)nd * fl;
+                const int j0 = world_index_at(h, (int)((long long)part * ctot / n_parts));
+                const int j1 = world_index_at(h, (int)((long long)(part + 1) * ctot / n_parts));
+                if (obstacles_vs_spheres<1, false>(sc, j0, j1, s, 1, flops))
+                    atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
             } else {
                 const int r = it - n_cw;
                 const int qq = r / nw, w = r - qq * nw;
@@ -607,18 +704,19 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
                 flops += kFlopPairExplicit;
             }
         }
-        __syncthreads();
+        g.sync();
     }
     // E: fine work items.  World: (obstacle chunk, sphere chunk, waypoint) with the
     // obstacle chunk slowest so a warp reads the same primitive (broadcast).
     // Self: (item, waypoint).
-    const int n_world = nw * h.n_sch * h.n_och;
-    const int n_total = n_world + nw * h.n_items;
+    const int n_world = nw * h.n_sch * n_parts;
+    const int n_self = nw * h.n_items;
+    const int n_total = n_world + n_self + (sc.pc.n > 0 ? nw * S : 0);
     for (int it = tid; it < n_total; it += T) {
         int w;
         bool hit = false;
         if (it < n_world) {
-            const int och = it / (nw * h.n_sch), r = it - och * (nw * h.n_sch);
+            const int part = it / (nw * h.n_sch), r = it - part * (nw * h.n_sch);
             const int si = r / nw;
             w = r - si * nw;
             if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) continue;
@@ -627,10 +725,16 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
             float4 s[kSphChunk];
 #pragma unroll
             for (int m = 0; m < kSphChunk; ++m) s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : far_sphere();
-            int nd, fl;
-            hit = full_sweep ? obstacles_vs_spheres<kSphChunk, true>(sc, och, s, nd, fl)
-                             : obstacles_vs_spheres<kSphChunk, false>(sc, och, s, nd, fl);
-            flops += (unsigned long long)nd * fl * ch.y;
+            const int j0 = world_index_at(h, (int)((long long)part * ctot / n_parts));
+            const int j1 = world_index_at(h, (int)((long long)(part + 1) * ctot / n_parts));
+            hit = full_sweep ? obstacles_vs_spheres<kSphChunk, true>(sc, j0, j1, s, ch.y, flops)
+                             : obstacles_vs_spheres<kSphChunk, false>(sc, j0, j1, s, ch.y, flops);
+        } else if (it >= n_world + n_self) {  // point cloud: (sphere, waypoint)
+            const int r = it - n_world - n_self;
+            const int si = r / nw;
+            w = r - si * nw;
+            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) continue;
+            hit = pc_sphere_hits(sc.pc, B.ctr[w * S_pad + si], full_sweep, flops);
         } else {
             const int r = it - n_world;
             const int ii = r / nw;
@@ -691,7 +795,7 @@ __device__ inline uint32_t cc_chunk(const Scene& sc, const CcBufs& B, int nw, bo
         for (int off = 16; off > 0; off >>= 1) flops += __shfl_xor_sync(0xffffffffu, flops, off);
         if ((tid & 31) == 0 && flops) atomicAdd(&B.stats[kStatFlops], flops);
     }
-    __syncthreads();
+    g.sync();
     return *vhit;
 }
 

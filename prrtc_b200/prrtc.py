@@ -15,9 +15,15 @@ Differences from the reference, all deliberate:
     consumers slice by tree size exactly as the reference's results do;
   * extra keyword-only arguments: ``edge_resolution`` (raise the waypoints of an
     edge to ceil(len/res)), ``threads_per_explorer``, ``waypoint_chunk``;
-    ``prrtc_plan_batch`` also takes ``goal_counts``, ``problem_order`` and
+    ``prrtc_plan_batch`` also takes ``goal_counts``, ``problem_order``,
     ``launch`` ("persistent" -- one persistent launch; "per_problem" -- one
-    planner launch per problem over a pool of streams, the reference's form).
+    planner launch per problem over a pool of streams, the reference's form),
+    ``tail_explorers`` (persistent launch: idle CTAs join problems that are
+    still running once every explorer slot is taken; False keeps exactly
+    ``num_new_samples`` explorers per problem, as the reference), and
+    ``point_cloud`` / ``r_env`` (an environment point cloud checked inside the
+    kernel, shared by the batch; a collision_context's ``point_cloud`` entry
+    does the same).
 """
 from __future__ import annotations
 
@@ -110,8 +116,10 @@ def _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio,
     return a
 
 
-def _tuning(edge_resolution=0.0, threads_per_explorer=0, waypoint_chunk=0, resident_ctas=0) -> _lib.Tuning:
+def _tuning(edge_resolution=0.0, threads_per_explorer=0, waypoint_chunk=0, resident_ctas=0,
+            tail_explorers=True) -> _lib.Tuning:
     t = _lib.Tuning()
+    t.tail_explorers = 0 if tail_explorers else -1
     t.edge_resolution = float(edge_resolution or 0.0)
     t.threads_per_explorer = int(threads_per_explorer or 0)
     t.waypoint_chunk = int(waypoint_chunk or 0)
@@ -170,8 +178,14 @@ class _Results:
         b[:, 10] = self.lengths
         b[:, 11] = self.costs.view(torch.int32)
 
-    def to_results(self, trees: bool = True) -> list[PRRTCResult]:
+    def to_results(self, trees: bool = True, paths_on_host: bool = False) -> list[PRRTCResult]:
+        """One read-back of the [B,16] scalar block (plus, with paths_on_host, one
+        bulk copy of every path) and the per-problem PRRTCResults."""
         host = self.block.cpu().numpy()
+        hpaths = None
+        if paths_on_host:
+            lmax = int(max(0, host[:, 10].max())) if self.B else 0
+            hpaths = self.paths[:, :lmax].cpu().numpy() if lmax > 0 else None
         out = []
         for i in range(self.B):
             row = host[i]
@@ -183,10 +197,12 @@ class _Results:
             path = None
             if solved:
                 if length > 0:
-                    path = self.paths[i, :length]
+                    path = torch.from_numpy(hpaths[i, :length]) if hpaths is not None else self.paths[i, :length]
                 else:  # longer than the device path buffer: walk on the host
                     path = self._host_trace(i)
                     cost = float(torch.linalg.norm(torch.diff(path, dim=0), dim=1).sum())
+                    if paths_on_host:
+                        path = path.cpu()
             ta = self.ta[i] if self.ta.dim() == 3 else self.ta
             tb = self.tb[i] if self.tb.dim() == 3 else self.tb
             pa = self.pa[i] if self.pa.dim() == 2 else self.pa
@@ -289,6 +305,11 @@ def prrtc_plan(
     attrs = _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
                    dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin)
     tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk)
+    from .pointcloud import cloud_from_context
+
+    cloud = cloud_from_context(collision_context, dev)  # optional "point_cloud" [M,3] + "r_env"
+    if cloud is not None:
+        tun.point_cloud = cloud.address()
     res = _Results(1, dim, int(max_nodes), dev, ())
     ws = workspace(lib.prrtc_b200_plan_workspace_size(C.byref(inp), C.byref(attrs), C.byref(tun)), dev)
     sp = stream_handle()
@@ -367,13 +388,18 @@ def prrtc_plan_batch(
     waypoint_chunk: int = 0,
     resident_ctas: int = 0,
     return_trees: bool = True,
+    paths_on_host: bool = False,
+    point_cloud=None,
+    r_env: float = 0.02,
+    tail_explorers: bool = True,
     device=None,
 ) -> list[PRRTCResult]:
     """Plan B independent problems (prrtc.py:882-1434).
 
     ``collision_context`` is one dict shared by every problem, or a list/tuple of
     per-problem dicts (robot tables from the first non-None entry; worlds and
-    self pairs packed into padded tensors with counts).
+    self pairs packed into padded tensors with counts).  ``paths_on_host``
+    returns every path as a CPU tensor, copied with one bulk device->host copy.
     """
     lib = _lib.load()
     collision_mode = _resolve_collision_mode(collision_checker)
@@ -457,7 +483,19 @@ def prrtc_plan_batch(
 
     attrs = _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
                    dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin)
-    tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk, resident_ctas)
+    tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk, resident_ctas, tail_explorers)
+    from .pointcloud import PointCloud, cloud_from_context
+
+    # one environment point cloud for the whole batch: a PointCloud, or the
+    # "point_cloud" entry of the first collision_context that has one
+    cloud = point_cloud if isinstance(point_cloud, PointCloud) else None
+    if cloud is None:
+        src = {"point_cloud": point_cloud, "r_env": r_env} if point_cloud is not None else next(
+            (c for c in contexts if c is not None and c.get("point_cloud") is not None), None)
+        cloud = cloud_from_context(src, dev)
+    if cloud is not None:
+        tun.point_cloud = cloud.address()
+        keep.append(cloud)
     res = _Results(B, dim, int(max_nodes), dev, (B,))
     sp = stream_handle()
     if launch == "persistent":
@@ -470,7 +508,7 @@ def prrtc_plan_batch(
     else:
         raise ValueError(f"launch must be 'persistent' or 'per_problem', got {launch!r}")
     res.extract(sp)
-    return res.to_results(trees=return_trees)
+    return res.to_results(trees=return_trees, paths_on_host=paths_on_host)
 
 
 def _plan_per_problem(lib, bi, res, attrs, tun, contexts, robot_ctx, starts, goals, goal_counts, lo, hi, dev,
@@ -542,3 +580,35 @@ def prrtc_extend(tree_configs, nearest_indices, samples, step_size):
     _lib.check(lib.prrtc_b200_extend(ptr(tree), dim, N, ptr(ni), ptr(s), B, ptr(st), ptr(out), ptr(par),
                                      ptr(valid), stream_handle()), "prrtc_b200_extend")
     return out, par, valid
+
+
+def prrtc_iteration(tree_a_configs: torch.Tensor, tree_b_configs: torch.Tensor, tree_a_parents: torch.Tensor,
+                    tree_b_parents: torch.Tensor, samples, tree_sizes: torch.Tensor, completed: torch.Tensor,
+                    step_size):
+    """Legacy single iteration (the "prrtc_iteration" target, prrtc_iteration.cu:180-277).
+
+    Updates the four tree tensors, ``tree_sizes`` and ``completed`` in place (CUDA
+    int32/float32 tensors, as the reference's kernel writes its input buffers)
+    and returns (new_configs as int32 float bits [batch, dim], new_parents,
+    valid_flags, solved_flag)."""
+    lib = _lib.load()
+    for name, t, dt in (("tree_a_configs", tree_a_configs, torch.float32), ("tree_b_configs", tree_b_configs,
+                        torch.float32), ("tree_a_parents", tree_a_parents, torch.int32),
+                        ("tree_b_parents", tree_b_parents, torch.int32), ("tree_sizes", tree_sizes, torch.int32),
+                        ("completed", completed, torch.int32)):
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != dt or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous CUDA {dt} tensor (updated in place)")
+    dev = tree_a_configs.device
+    dim, N = int(tree_a_configs.shape[0]), int(tree_a_configs.shape[1])
+    s = as_tensor(samples, torch.float32, dev).reshape(-1, dim)
+    B = int(s.shape[0])
+    st = as_tensor(np.array([step_size], dtype=np.float32).reshape(-1)[:1], torch.float32, dev)
+    new_cfg = torch.empty((B, dim), dtype=torch.int32, device=dev)
+    par = torch.empty((B,), dtype=torch.int32, device=dev)
+    valid = torch.empty((B,), dtype=torch.int32, device=dev)
+    solved = torch.empty((1,), dtype=torch.int32, device=dev)
+    _lib.check(lib.prrtc_b200_iteration(ptr(tree_a_configs), ptr(tree_b_configs), ptr(tree_a_parents),
+                                        ptr(tree_b_parents), dim, N, ptr(s), B, ptr(tree_sizes), ptr(completed),
+                                        ptr(st), ptr(new_cfg), ptr(par), ptr(valid), ptr(solved), stream_handle()),
+               "prrtc_b200_iteration")
+    return new_cfg, par, valid, solved

@@ -277,6 +277,33 @@ def uneven_world(rng) -> dict:
     return w
 
 
+def box_surface_points(rng, boxes: np.ndarray, n: int) -> np.ndarray:
+    """n points uniform over the surfaces of oriented boxes [Nb, 15] (c, a1, a2, a3, half-lengths)."""
+    boxes = np.asarray(boxes, np.float64).reshape(-1, 15)
+    hl = boxes[:, 12:15]
+    # faces of box b: axis k at +-hl[k], spanned by the two other axes
+    area = np.stack([4 * hl[:, 1] * hl[:, 2], 4 * hl[:, 0] * hl[:, 2], 4 * hl[:, 0] * hl[:, 1]], 1)  # [Nb, 3]
+    w = np.repeat(area, 2, axis=1).reshape(-1)
+    face = rng.choice(w.shape[0], size=n, p=w / w.sum())
+    b, k, sign = face // 6, (face % 6) // 2, np.where(face % 2 == 0, 1.0, -1.0)
+    u = rng.uniform(-1.0, 1.0, size=(n, 3))
+    u[np.arange(n), k] = sign
+    local = u * hl[b]
+    axes = boxes[b, 3:12].reshape(n, 3, 3)  # rows a1, a2, a3
+    return (boxes[b, :3] + np.einsum("nk,nkj->nj", local, axes)).astype(np.float32)
+
+
+def pointcloud_world(rng, n_points: int = 20000) -> tuple[dict, np.ndarray]:
+    """Tabletop scene whose 20 boxes are seen only as a scanned point cloud
+    (n_points on their surfaces); floor, capsules and spheres stay analytic."""
+    base = tabletop_world(rng)
+    pts = box_surface_points(rng, base["world_boxes"], n_points)
+    w = empty_world()
+    for k in ("world_spheres", "world_capsules", "world_halfspaces"):
+        w[k] = base[k]
+    return w, pts
+
+
 LARGE_LO, LARGE_HI = (-2.4, -2.6, 0.0), (2.4, 2.6, 2.0)
 
 
@@ -327,7 +354,7 @@ BUCKETS = (4096, 16384, 65536)
 
 
 def make_problem(kind: str, seed: int, checker: Checker, robot: RobotModel | None = None) -> Problem:
-    """Problem ``seed`` of workload ``kind``: spheres16 | tabletop | uneven | large."""
+    """Problem ``seed`` of workload ``kind``: spheres16 | tabletop | uneven | large | pointcloud."""
     rng = np.random.default_rng(seed)
     if kind == "large":
         robot = robot or dual_arm(0)
@@ -346,9 +373,14 @@ def make_problem(kind: str, seed: int, checker: Checker, robot: RobotModel | Non
         world = large_world(rng)
         n_goals = int(rng.integers(1, 5))
         max_nodes = 131072
+    elif kind == "pointcloud":
+        world, cloud = pointcloud_world(rng)
+        n_goals, max_nodes = 2, 65536
     else:
         raise ValueError(f"unknown workload {kind!r}")
     ctx = build_collision_context(robot, world)
+    if kind == "pointcloud":
+        ctx["point_cloud"], ctx["r_env"] = cloud, 0.01
     lo, hi = robot.lower.astype(np.float32), robot.upper.astype(np.float32)
     qs = sample_free(rng, ctx, lo, hi, 1 + n_goals, checker)
     return Problem(seed, ctx, qs[0], qs[1:], lo, hi, max_nodes)

@@ -25,6 +25,12 @@ STEP_TRIALS = 48
 CONNECT_TRIALS = 48
 
 
+def halton_bounds(dim):
+    """Sampling bounds of the Halton vectors (float32, made on the host so the
+    generator and the test use the same bits)."""
+    return np.full(dim, -2.8, np.float32), np.linspace(1.0, 3.0, dim).astype(np.float32)
+
+
 def step_inputs(k):
     rng = np.random.default_rng(1000 + k)
     dim = 7 if k % 3 else 14
@@ -65,8 +71,9 @@ def main(out):
         orders.append(po.cpu().numpy().copy())
     res["prime_orders"] = np.stack(orders)
     for dim in (7, 14):
-        lo = torch.full((dim,), -2.8, device=dev)
-        hi = torch.linspace(1.0, 3.0, dim, device=dev)
+        lo_h, hi_h = halton_bounds(dim)
+        res[f"halton_lo_dim{dim}"], res[f"halton_hi_dim{dim}"] = lo_h, hi_h
+        lo, hi = torch.from_numpy(lo_h).to(dev), torch.from_numpy(hi_h).to(dev)
         outs = []
         for e in HALTON_EXPLORERS:
             o = torch.empty((HALTON_N, dim), device=dev)

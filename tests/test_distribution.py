@@ -3,6 +3,8 @@ oracle's sequential restatement of the same algorithm.
 
 Explorers race on the GPU, so trees differ run to run (the reference says the
 same: verify_coarse_equivalence.py:3-8); what must agree are the distributions.
+The batched planner runs with exactly num_new_samples explorers per problem
+(tail_explorers=False), as the reference and the oracle do.
 Criteria, at 95%: the Wilson intervals of the two success rates overlap, and the
 bootstrap intervals of the two median path costs overlap.  Every GPU path is
 re-validated with the float64 binary checker at 0.01 rad.
@@ -67,7 +69,7 @@ def test_success_and_cost_distributions_match_oracle(cuda, orc):
     res = prrtc_plan_batch(np.stack([p.start for p in problems]), np.stack([p.goals for p in problems]),
                            max_nodes=N_NODES, min_vals=problems[0].lower, max_vals=problems[0].upper,
                            collision_context=[p.context for p in problems], collision_checker=CHECKER,
-                           edge_resolution=RES, return_trees=False, **SETTINGS)
+                           edge_resolution=RES, return_trees=False, tail_explorers=False, **SETTINGS)
     gs = np.array([r.solved for r in res])
     gc = np.array([r.cost for r in res if r.solved])
     os_ = np.array([s for s, _ in ora])

@@ -35,8 +35,7 @@ def test_prime_orders(orc, gold):
 
 @pytest.mark.parametrize("dim", [7, 14])
 def test_halton_samples(orc, gold, dim):
-    lo = np.full(dim, -2.8, np.float32)
-    hi = np.linspace(1.0, 3.0, dim).astype(np.float32)
+    lo, hi = gold[f"halton_lo_dim{dim}"], gold[f"halton_hi_dim{dim}"]
     for i, e in enumerate(HALTON_EXPLORERS):
         assert np.array_equal(bits(orc.halton_samples(e, HALTON_N, lo, hi)), bits(gold[f"halton_dim{dim}"][i])), e
 

@@ -124,13 +124,16 @@ def test_reference_connect_pins_oracle(cuda, orc):
         assert np.array_equal(_bits(vec.cpu().numpy()), _bits(want))
 
 
-def test_nearest_neighbor_matches_oracle_and_reference(cuda, orc):
+@pytest.mark.parametrize("batch", [1, 5, 13, 64])
+def test_nearest_neighbor_matches_oracle_and_reference(cuda, orc, batch):
+    """batch >= 4 with a tree row length divisible by 4 takes the query-tiled
+    kernel (8 queries per tile, ragged last tile); the rest the per-query one."""
     from prrtc_b200 import prrtc_nearest_neighbor
 
-    rng = np.random.default_rng(7)
-    for dim, N, n in ((7, 65536, 50000), (14, 8192, 8192), (3, 4099, 4000)):
+    rng = np.random.default_rng(7 + batch)
+    for dim, N, n in ((7, 65536, 50000), (14, 8192, 8192), (3, 4099, 4000), (16, 4096, 4093)):
         tree = _random_tree(rng, dim, N, n)
-        q = rng.uniform(-2.8, 2.8, (64, dim)).astype(np.float32)
+        q = rng.uniform(-2.8, 2.8, (batch, dim)).astype(np.float32)
         tt, tq = torch.from_numpy(tree).to(cuda), torch.from_numpy(q).to(cuda)
         dist, idx = prrtc_nearest_neighbor(tt, tq, n)
         oi, od = orc.nearest_batch(tree, n, q)
@@ -138,9 +141,9 @@ def test_nearest_neighbor_matches_oracle_and_reference(cuda, orc):
         assert np.array_equal(_bits(dist.cpu().numpy()), _bits(np.sqrt(od.astype(np.float32))))
         if REF_LIB.exists():
             ref = _ref()
-            ri = torch.empty(64, dtype=torch.int32, device=cuda)
-            rd = torch.empty(64, device=cuda)
-            assert ref.ref_nn(tt.data_ptr(), dim, N, n, tq.data_ptr(), 64, ri.data_ptr(),
+            ri = torch.empty(batch, dtype=torch.int32, device=cuda)
+            rd = torch.empty(batch, device=cuda)
+            assert ref.ref_nn(tt.data_ptr(), dim, N, n, tq.data_ptr(), batch, ri.data_ptr(),
                               rd.data_ptr(), _s()) == 0
             assert np.array_equal(ri.cpu().numpy(), oi)  # random floats: no ties
             assert np.array_equal(_bits(rd.cpu().numpy()), _bits(dist.cpu().numpy()))
@@ -153,12 +156,14 @@ def test_nearest_neighbor_ties_lowest_index(cuda, orc):
     rng = np.random.default_rng(11)
     base = rng.uniform(-1, 1, (dim, 37)).astype(np.float32)
     tree = np.tile(base, (1, N // 37 + 1))[:, :N].copy()
-    q = base[:, [3, 5, 36]].T.copy()
-    dist, idx = prrtc_nearest_neighbor(torch.from_numpy(tree).to(cuda), torch.from_numpy(q).to(cuda), N)
-    assert idx.cpu().tolist() == [3, 5, 36]
-    assert np.all(dist.cpu().numpy() == 0.0)
-    oi, _ = orc.nearest_batch(tree, N, q)
-    assert oi.tolist() == [3, 5, 36]
+    cols = [3, 5, 36, 0, 1, 2, 4, 6, 7, 8, 30]  # 11 queries: the query-tiled kernel
+    for sel in (cols[:3], cols):
+        q = base[:, sel].T.copy()
+        dist, idx = prrtc_nearest_neighbor(torch.from_numpy(tree).to(cuda), torch.from_numpy(q).to(cuda), N)
+        assert idx.cpu().tolist() == sel
+        assert np.all(dist.cpu().numpy() == 0.0)
+        oi, _ = orc.nearest_batch(tree, N, q)
+        assert oi.tolist() == sel
 
 
 def test_extend_matches_reference(cuda, orc):
@@ -270,8 +275,11 @@ def test_plan_solves_and_revalidates(cuda, orc, kind, seed, checker):
     _check_tree_sound(sc, r.tree_b_configs.cpu().numpy(), r.tree_b_parents.cpu().numpy(), r.tree_b_size, pr.dim)
 
 
-@pytest.mark.parametrize("launch", ["persistent", "per_problem"])
-def test_batch_uneven_solves(cuda, orc, launch):
+@pytest.mark.parametrize("launch,threads", [("persistent", 128), ("persistent", 32), ("per_problem", 128),
+                                            ("per_problem", 32)])
+def test_batch_uneven_solves(cuda, orc, launch, threads):
+    """threads=32 with the persistent launch runs one explorer per warp, four
+    explorers of a problem per CTA."""
     from prrtc_b200 import prrtc_plan_batch
 
     probs = [make_problem("uneven", 100 + i) for i in range(12)]
@@ -283,8 +291,40 @@ def test_batch_uneven_solves(cuda, orc, launch):
     res = prrtc_plan_batch(np.stack([p.start for p in probs]), goals, max_iterations=5000, num_new_samples=32,
                            max_nodes=16384, min_vals=probs[0].lower, max_vals=probs[0].upper,
                            collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
-                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01, launch=launch)
+                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01, launch=launch,
+                           threads_per_explorer=threads)
     assert len(res) == len(probs)
+    assert sum(r.solved for r in res) >= len(probs) - 1
+    for i, (p, r) in enumerate(zip(probs, res)):
+        if not r.solved:
+            continue
+        path = r.path.cpu().numpy()
+        assert np.array_equal(path[0], p.start)
+        assert any(np.array_equal(path[-1], g) for g in p.goals)
+        sc = orc.Scene(p.context, dim)
+        ok, md = sc.validate_path(path, 0.01)
+        assert ok, md
+        if i < 3:
+            _check_tree_sound(sc, r.tree_a_configs.cpu().numpy(), r.tree_a_parents.cpu().numpy(), r.tree_a_size, dim)
+            _check_tree_sound(sc, r.tree_b_configs.cpu().numpy(), r.tree_b_parents.cpu().numpy(), r.tree_b_size, dim)
+
+
+def test_batch_dual_arm_large_world(cuda, orc):
+    """Dual-arm workload: 14 joints (18 with 4 mimic gripper joints), 120
+    spheres, 256 spheres + 64 boxes + floor, 131072-node trees, 1-4 goals."""
+    from prrtc_b200 import prrtc_plan_batch
+
+    probs = [make_problem("large", 300 + i) for i in range(6)]
+    G = max(p.goals.shape[0] for p in probs)
+    dim = probs[0].dim
+    assert dim == 14
+    goals = np.zeros((len(probs), G, dim), np.float32)
+    for i, p in enumerate(probs):
+        goals[i, : p.goals.shape[0]] = p.goals
+    res = prrtc_plan_batch(np.stack([p.start for p in probs]), goals, max_iterations=10000, num_new_samples=64,
+                           max_nodes=131072, min_vals=probs[0].lower, max_vals=probs[0].upper,
+                           collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
+                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01)
     assert sum(r.solved for r in res) >= len(probs) - 1
     for p, r in zip(probs, res):
         if not r.solved:
@@ -294,3 +334,43 @@ def test_batch_uneven_solves(cuda, orc, launch):
         assert any(np.array_equal(path[-1], g) for g in p.goals)
         ok, md = orc.Scene(p.context, dim).validate_path(path, 0.01)
         assert ok, md
+
+
+@pytest.mark.parametrize("N,batch", [(1024, 64), (4, 10)])
+def test_legacy_iteration_matches_oracle(cuda, orc, N, batch):
+    """prrtc_iteration: reset to one node per tree, then every sample extends
+    tree (sample & 1) from its root into slot 1 + sample // 2 (bit-exact
+    candidates; slots past max_nodes are invalid and not counted)."""
+    from prrtc_b200 import prrtc_iteration
+
+    rng = np.random.default_rng(N + batch)
+    dim = 7
+    ta = np.full((dim, N), np.nan, np.float32)
+    tb = np.full((dim, N), np.nan, np.float32)
+    ta[:, 0] = rng.uniform(-1, 1, dim)
+    tb[:, 0] = rng.uniform(-1, 1, dim)
+    samples = rng.uniform(-2.8, 2.8, (batch, dim)).astype(np.float32)
+    step = 0.5
+    tta, ttb = torch.from_numpy(ta).to(cuda), torch.from_numpy(tb).to(cuda)
+    pa = torch.full((N,), -1, dtype=torch.int32, device=cuda)
+    pb = torch.full((N,), -1, dtype=torch.int32, device=cuda)
+    sizes = torch.tensor([7, 9], dtype=torch.int32, device=cuda)  # reset by the call
+    comp = torch.tensor([7, 9], dtype=torch.int32, device=cuda)
+    cfg, par, valid, solved = prrtc_iteration(tta, ttb, pa, pb, samples, sizes, comp, step)
+    cfg = cfg.cpu().numpy()
+    trees = [ta, tb]
+    n_t = [(batch + 1) // 2, batch // 2]
+    assert sizes.cpu().tolist() == [1 + min(n_t[0], N - 1), 1 + min(n_t[1], N - 1)]
+    assert comp.cpu().tolist() == sizes.cpu().tolist() and solved.item() == 0
+    out = [tta.cpu().numpy(), ttb.cpu().numpy()]
+    outp = [pa.cpu().numpy(), pb.cpu().numpy()]
+    for b in range(batch):
+        t = b & 1
+        idx, dsq = orc.nearest(trees[t], 1, samples[b])
+        assert idx == 0
+        cand = orc.extend(trees[t][:, 0], samples[b], float(np.sqrt(np.float32(dsq), dtype=np.float32)), step)
+        assert np.array_equal(cfg[b], np.ascontiguousarray(cand, np.float32).view(np.int32))
+        slot = 1 + b // 2
+        assert valid[b].item() == int(slot < N) and par[b].item() == 0
+        if slot < N:
+            assert np.array_equal(out[t][:, slot].view(np.int32), cfg[b]) and outp[t][slot] == 0

@@ -292,3 +292,32 @@ def test_smooth_cost_finite_difference_consistency(orc):
     assert np.isfinite(c) and c > 0
     w2 = w.copy(); w2[3, 2] += 1e-3
     assert sc.smooth_cost(w2, 0.02, 50.0, 1.0) != c
+
+
+def test_point_cloud_stage_brute_force(orc, arm):
+    """The oracle's point-cloud stage: a sphere hits a point iff |c - p| <= r + r_env."""
+    from prrtc_b200.scenes import box_surface_points
+
+    rng = np.random.default_rng(3)
+    boxes = np.array([[0.5, 0.0, 0.5, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0.2, 0.3, 0.1]], np.float32)
+    pts = box_surface_points(rng, boxes, 3000)
+    # every point on the box surface: one local coordinate at +-half-length
+    loc = np.abs(pts - boxes[0, :3]) / boxes[0, 12:15]
+    assert np.allclose(loc.max(1), 1.0, atol=1e-5) and (loc <= 1.0 + 1e-5).all()
+    ctx = build_collision_context(arm, empty_world())
+    for k in ("self_pairs",):
+        ctx.pop(k, None)
+    ctx["point_cloud"], ctx["r_env"] = pts, 0.02
+    sc = orc.Scene(ctx, arm.dim)
+    q = rng.uniform(arm.lower, arm.upper, (60, arm.dim)).astype(np.float32)
+    v = sc.check_configs(q, 0)
+    md = sc.min_distances(q)
+    for i in range(q.shape[0]):
+        F = sc.fk(q[i])  # [J, 12]
+        c = np.einsum("sij,sj->si", F[ctx["sphere_link_idx"], :9].reshape(-1, 3, 3), ctx["sphere_local"]) + \
+            F[ctx["sphere_link_idx"], 9:]
+        d = np.linalg.norm(c[:, None, :] - pts[None].astype(np.float64), axis=-1) - ctx["sphere_radius"][:, None] - 0.02
+        assert abs(d.min() - md[i]) < 1e-6
+        if abs(d.min()) > 1e-6:
+            assert v[i] == int(d.min() <= 0)
+    assert 0 < v.sum() < q.shape[0]
