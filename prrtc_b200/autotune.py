@@ -17,9 +17,9 @@ from pathlib import Path
 
 import torch
 
-SAMPLES = (4, 8, 16, 32, 64)
-THREADS = (32, 64, 128)
-CHUNKS = (8, 16)
+SAMPLES = (1, 2, 4, 8, 16)
+THREADS = (64, 128)  # 32 (one explorer per warp) stays available but lost on every bucket measured
+CHUNKS = (8, 16, 32)
 CANDIDATES = tuple((e, t, c) for t in THREADS for c in CHUNKS for e in SAMPLES)
 CACHE = Path(os.environ.get("PRRTC_B200_CACHE", Path.home() / ".cache" / "prrtc_b200")) / "autotune.json"
 
@@ -42,7 +42,7 @@ def choose(problems, N: int, settings, dev, candidates=CANDIDATES, use_cache: bo
     """Best {num_new_samples, threads_per_explorer, waypoint_chunk} for this bucket."""
     from .batch import BatchPlanner, PlanSettings
 
-    key = "v4|" + _key(dev, N, problems, settings)
+    key = "v5|" + _key(dev, N, problems, settings)
     cache = _load() if use_cache else {}
     if key in cache:
         return dict(cache[key])

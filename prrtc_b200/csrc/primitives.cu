@@ -177,7 +177,8 @@ cudaError_t launch_nearest(const float* tree, int dim, int N, const int32_t* tre
     constexpr int kQT = 8;
     const bool tiled = batch >= 4 && (N & 3) == 0 && (reinterpret_cast<uintptr_t>(tree) & 15) == 0;
     const int tiles = tiled ? (batch + kQT - 1) / kQT : batch;
-    int splits = std::max(1, (4 * sms + tiles - 1) / tiles);
+    // 8 CTAs of 256 threads per SM keep enough loads in flight to stream a tree from HBM
+    int splits = std::max(1, (8 * sms + tiles - 1) / tiles);
     int slice = (N + splits - 1) / splits;
     slice = std::max(1024, (slice + 1023) & ~1023);
     splits = (N + slice - 1) / slice;
@@ -297,7 +298,7 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 #define PRRTC_CHECK_CW 32       // configurations per CTA pass of the batched checker
 #endif
 #ifndef PRRTC_CHECK_MINBLOCKS
-#define PRRTC_CHECK_MINBLOCKS 5 // resident CTAs per SM the register allocation must allow
+#define PRRTC_CHECK_MINBLOCKS 4 // resident CTAs per SM the register allocation must allow (shared memory allows 4 at CW 32)
 #endif
 
 template <int CW>

@@ -37,7 +37,7 @@ constexpr float kFar = 1.0e18f;  // centre of a sphere that can never collide
 
 // FP32 operations per primitive test as issued by the functions below (FFMA = 2,
 // FADD/FMUL = 1; min/max/abs and the MUFU of sin/cos/sqrt are not counted).
-constexpr int kFlopSphere = 8, kFlopCapsule = 23, kFlopBox = 27, kFlopHalfspace = 7;
+constexpr int kFlopSphere = 8, kFlopCapsule = 23, kFlopBox = 26, kFlopHalfspace = 6;
 constexpr int kFlopPair = 8, kFlopPairExplicit = 11;
 constexpr int kFlopXform = 18;                  // one sphere centre
 constexpr int kFlopJointLocal = 90, kFlopJointChain = 63;
@@ -402,28 +402,31 @@ __device__ __forceinline__ float4 xform_point(const float* F, float4 l) {
 // g = A + c.O, and the pair collides iff g <= -B.
 __device__ __forceinline__ float sphere_A(float4 c) { return fmaf(c.x, c.x, fmaf(c.y, c.y, fmaf(c.z, c.z, -c.w * c.w))); }
 
-// Minimum of NS values as a tree (depth log2 NS instead of a serial chain).
-template <int NS>
-__device__ __forceinline__ float tree_min(float (&v)[NS]) {
-#pragma unroll
-    for (int w = 1; w < NS; w *= 2)
-#pragma unroll
-        for (int k = 0; k + w < NS; k += 2 * w) v[k] = fminf(v[k], v[k + w]);
-    return v[0];
+// Per-sphere running minima.  Each test below returns a value h whose
+// comparison with a per-sphere threshold decides a hit; a work item keeps one
+// running minimum per sphere over all obstacles of a type (independent FFMA
+// chains, no cross-sphere reduction per obstacle) and compares once per group
+// of obstacles:
+//   sphere     h = B + O.(c, r)        (O = -2(o, r_o), B = |o|^2 - r_o^2),  hit iff h <= -(|c|^2 - r^2)
+//   capsule    h = |e|^2 - (r + r_c)^2 (e = c - p1 - t d, t = sat(d'.c + off)), hit iff h <= 0
+//   box        h = |max(|l| - hl, 0)|^2 (l = box-frame coordinates),         hit iff h <= r^2
+//   halfspace  h = n.c - n.p                                                  hit iff h <= r
+// Three-input minimum (PTX min.f32 with three sources, sm_100): folds two
+// obstacles into a running minimum with one instruction.
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
 }
 
 template <int NS>
-__device__ __forceinline__ float min_sphere(const float4 (&c)[NS], const float (&A)[NS], float4 O) {
-    float g[NS];
+__device__ __forceinline__ void h_sphere(float (&h)[NS], const float4 (&c)[NS], float4 O, float B) {
 #pragma unroll
-    for (int k = 0; k < NS; ++k) g[k] = fmaf(c[k].x, O.x, fmaf(c[k].y, O.y, fmaf(c[k].z, O.z, fmaf(c[k].w, O.w, A[k]))));
-    return tree_min<NS>(g);
+    for (int k = 0; k < NS; ++k) h[k] = fmaf(c[k].x, O.x, fmaf(c[k].y, O.y, fmaf(c[k].z, O.z, fmaf(c[k].w, O.w, B))));
 }
 
-// Capsule: t = sat(d'.c + off), e = (c - p1) - t d, g = |e|^2 - (rc + r)^2.
 template <int NS>
-__device__ __forceinline__ float min_capsule(const float4 (&c)[NS], float4 p1r, float4 dp, float4 d) {
-    float g[NS];
+__device__ __forceinline__ void h_capsule(float (&h)[NS], const float4 (&c)[NS], float4 p1r, float4 dp, float4 d) {
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
         const float t = __saturatef(fmaf(dp.x, c[k].x, fmaf(dp.y, c[k].y, fmaf(dp.z, c[k].z, dp.w))));
@@ -431,34 +434,52 @@ __device__ __forceinline__ float min_capsule(const float4 (&c)[NS], float4 p1r, 
         const float ey = fmaf(-t, d.y, c[k].y - p1r.y);
         const float ez = fmaf(-t, d.z, c[k].z - p1r.z);
         const float s = c[k].w + p1r.w;
-        g[k] = fmaf(ex, ex, fmaf(ey, ey, fmaf(ez, ez, -s * s)));
+        h[k] = fmaf(ex, ex, fmaf(ey, ey, fmaf(ez, ez, -s * s)));
     }
-    return tree_min<NS>(g);
 }
 
-// Oriented box: l_k = a_k.c + off_k (box-frame coordinates), q_k = max(|l_k| - h_k, 0),
-// g = |q|^2 - r^2 (nR2 = -r^2 per sphere).  Inside the box g = -r^2 <= 0.
 template <int NS>
-__device__ __forceinline__ float min_box(const float4 (&c)[NS], const float (&nR2)[NS], float4 a1, float4 a2,
-                                         float4 a3, float4 h) {
-    float g[NS];
+__device__ __forceinline__ void h_box(float (&h)[NS], const float4 (&c)[NS], float4 a1, float4 a2, float4 a3,
+                                      float4 hl) {
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-        const float q1 = fmaxf(fabsf(fmaf(a1.x, c[k].x, fmaf(a1.y, c[k].y, fmaf(a1.z, c[k].z, a1.w)))) - h.x, 0.0f);
-        const float q2 = fmaxf(fabsf(fmaf(a2.x, c[k].x, fmaf(a2.y, c[k].y, fmaf(a2.z, c[k].z, a2.w)))) - h.y, 0.0f);
-        const float q3 = fmaxf(fabsf(fmaf(a3.x, c[k].x, fmaf(a3.y, c[k].y, fmaf(a3.z, c[k].z, a3.w)))) - h.z, 0.0f);
-        g[k] = fmaf(q1, q1, fmaf(q2, q2, fmaf(q3, q3, nR2[k])));
+        const float q1 = fmaxf(fabsf(fmaf(a1.x, c[k].x, fmaf(a1.y, c[k].y, fmaf(a1.z, c[k].z, a1.w)))) - hl.x, 0.0f);
+        const float q2 = fmaxf(fabsf(fmaf(a2.x, c[k].x, fmaf(a2.y, c[k].y, fmaf(a2.z, c[k].z, a2.w)))) - hl.y, 0.0f);
+        const float q3 = fmaxf(fabsf(fmaf(a3.x, c[k].x, fmaf(a3.y, c[k].y, fmaf(a3.z, c[k].z, a3.w)))) - hl.z, 0.0f);
+        h[k] = fmaf(q1, q1, fmaf(q2, q2, q3 * q3));
     }
-    return tree_min<NS>(g);
 }
 
-// Halfspace: g = n.c - n.p - r.
 template <int NS>
-__device__ __forceinline__ float min_halfspace(const float4 (&c)[NS], float4 hs) {
-    float g[NS];
+__device__ __forceinline__ void h_halfspace(float (&h)[NS], const float4 (&c)[NS], float4 hs) {
 #pragma unroll
-    for (int k = 0; k < NS; ++k) g[k] = fmaf(hs.x, c[k].x, fmaf(hs.y, c[k].y, fmaf(hs.z, c[k].z, hs.w))) - c[k].w;
-    return tree_min<NS>(g);
+    for (int k = 0; k < NS; ++k) h[k] = fmaf(hs.x, c[k].x, fmaf(hs.y, c[k].y, fmaf(hs.z, c[k].z, hs.w)));
+}
+
+template <int NS>
+__device__ __forceinline__ void fold1(float (&m)[NS], const float (&h)[NS]) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) m[k] = fminf(m[k], h[k]);
+}
+
+template <int NS>
+__device__ __forceinline__ void fold2(float (&m)[NS], const float (&h1)[NS], const float (&h2)[NS]) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) m[k] = fmin3(m[k], h1[k], h2[k]);
+}
+
+template <int NS>
+__device__ __forceinline__ bool any_le(const float (&m)[NS], const float (&thr)[NS]) {
+    bool r = false;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) r |= m[k] <= thr[k];
+    return r;
+}
+
+template <int NS>
+__device__ __forceinline__ void fill(float (&m)[NS], float v) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) m[k] = v;
 }
 
 __device__ __forceinline__ float4 far_sphere() { return make_float4(kFar, kFar, kFar, 0.0f); }
@@ -489,59 +510,95 @@ __device__ __forceinline__ int world_index_at(const BlobHeader& h, int x) {
 
 // Obstacles [j0, j1) of the combined list against NS sphere centres held in
 // registers (c.w = radius + inflation; padding spheres sit at kFar).  FULL:
-// test every obstacle without a per-obstacle branch; otherwise return at the
-// first hit.  flops accumulates the FP32 flops of the tests executed (NS_real
-// real spheres per test).
+// test every obstacle; otherwise stop at the first group of kHitCheck
+// obstacles that holds a hit.  flops accumulates the FP32 flops of the tests
+// executed (NS_real real spheres per test).
+constexpr int kHitCheck = 8;
+
+// One sphere chunk against obstacles [lo, hi) of one type: running minimum per
+// sphere; FULL folds two obstacles per three-input minimum, !FULL one obstacle
+// at a time with a hit check every kHitCheck obstacles.  Returns whether some sphere reached its threshold;
+// `done` = obstacles tested.
+template <int NS, bool FULL, class Test>
+__device__ __forceinline__ bool sweep_type(float (&m)[NS], const float (&thr)[NS], int lo, int hi, Test test,
+                                           int& done) {
+    fill(m, INFINITY);
+    int o = lo;
+    if constexpr (FULL) {  // throughput form: two obstacles per fold
+        for (; o + 1 < hi; o += 2) {
+            float h1[NS], h2[NS];
+            test(h1, o);
+            test(h2, o + 1);
+            fold2(m, h1, h2);
+        }
+    } else {  // early-exit form (inside the planner): fewer live registers
+        for (; o < hi; ++o) {
+            float h1[NS];
+            test(h1, o);
+            fold1(m, h1);
+            if (((o - lo) & (kHitCheck - 1)) == kHitCheck - 1 && any_le(m, thr)) {
+                done = o + 1 - lo;
+                return true;
+            }
+        }
+    }
+    if (o < hi) {
+        float h1[NS];
+        test(h1, o);
+        fold1(m, h1);
+    }
+    done = hi - lo;
+    return any_le(m, thr);
+}
+
 template <int NS, bool FULL>
 __device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int j0, int j1, const float4 (&s)[NS],
                                                      int ns_real, unsigned long long& flops) {
     const BlobHeader& h = *sc.h;
-    float best = INFINITY;  // minimum margin value seen (<= 0 means a hit)
+    float m[NS], thr[NS];
+    bool hit = false;
+    int done = 0;
     int lo = max(j0, 0), hi = min(j1, h.Ns);
     if (lo < hi) {
-        float A[NS];
 #pragma unroll
-        for (int k = 0; k < NS; ++k) A[k] = sphere_A(s[k]);
-        for (int o = lo; o < hi; ++o) {
-            best = fminf(best, min_sphere<NS>(s, A, sc.ws[2 * o]) + sc.ws[2 * o + 1].w);
-            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopSphere; return true; }
-        }
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopSphere;
+        for (int k = 0; k < NS; ++k) thr[k] = -sphere_A(s[k]);
+        const float4* ws = sc.ws;
+        hit |= sweep_type<NS, FULL>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_sphere<NS>(v, s, ws[2 * o], ws[2 * o + 1].w); }, done);
+        flops += (unsigned long long)done * ns_real * kFlopSphere;
+        if (!FULL && hit) return true;
     }
     int base = h.Ns;
     lo = max(j0, base) - base;
     hi = min(j1, base + h.Nc) - base;
     if (lo < hi) {
-        for (int o = lo; o < hi; ++o) {
-            best = fminf(best, min_capsule<NS>(s, sc.wc[3 * o], sc.wc[3 * o + 1], sc.wc[3 * o + 2]));
-            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopCapsule; return true; }
-        }
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopCapsule;
+        fill(thr, 0.0f);
+        const float4* wc = sc.wc;
+        hit |= sweep_type<NS, FULL>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_capsule<NS>(v, s, wc[3 * o], wc[3 * o + 1], wc[3 * o + 2]); }, done);
+        flops += (unsigned long long)done * ns_real * kFlopCapsule;
+        if (!FULL && hit) return true;
     }
     base += h.Nc;
     lo = max(j0, base) - base;
     hi = min(j1, base + h.Nb) - base;
     if (lo < hi) {
-        float nR2[NS];
 #pragma unroll
-        for (int k = 0; k < NS; ++k) nR2[k] = -s[k].w * s[k].w;
-        for (int o = lo; o < hi; ++o) {
-            best = fminf(best, min_box<NS>(s, nR2, sc.wb[4 * o], sc.wb[4 * o + 1], sc.wb[4 * o + 2], sc.wb[4 * o + 3]));
-            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopBox; return true; }
-        }
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopBox;
+        for (int k = 0; k < NS; ++k) thr[k] = s[k].w * s[k].w;
+        const float4* wb = sc.wb;
+        hit |= sweep_type<NS, FULL>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_box<NS>(v, s, wb[4 * o], wb[4 * o + 1], wb[4 * o + 2], wb[4 * o + 3]); }, done);
+        flops += (unsigned long long)done * ns_real * kFlopBox;
+        if (!FULL && hit) return true;
     }
     base += h.Nb;
     lo = max(j0, base) - base;
     hi = min(j1, base + h.Nh) - base;
     if (lo < hi) {
-        for (int o = lo; o < hi; ++o) {
-            best = fminf(best, min_halfspace<NS>(s, sc.wh[o]));
-            if (!FULL && best <= 0.0f) { flops += (unsigned long long)(o - lo + 1) * ns_real * kFlopHalfspace; return true; }
-        }
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopHalfspace;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) thr[k] = s[k].w;
+        const float4* wh = sc.wh;
+        hit |= sweep_type<NS, true>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_halfspace<NS>(v, s, wh[o]); }, done);
+        flops += (unsigned long long)done * ns_real * kFlopHalfspace;
     }
-    return best <= 0.0f;
+    return hit;
 }
 
 // ----------------------------------------------------------------------------- thread groups
@@ -574,8 +631,11 @@ struct CcBufs {
     uint32_t* dirty; // [CW][KW]
     uint32_t* gate;  // [CW][QW]
     uint32_t* hit;   // [1]
+    int* bounds;     // [kMaxParts + 1] first obstacle of each world part
     unsigned long long* stats;  // optional device counters (kStat*), may be null
 };
+
+constexpr int kMaxParts = 256;  // world parts per chunk (cost-balanced obstacle ranges)
 
 __host__ __device__ inline int cc_smem_bytes(int J, int S, int K, int Q, int CW) {
     const int S_pad = odd_pad(S);
@@ -588,6 +648,7 @@ __host__ __device__ inline int cc_smem_bytes(int J, int S, int K, int Q, int CW)
     b += align16(CW * KW * 4);
     b += align16(CW * QW * 4);
     b += 16;
+    b += align16((kMaxParts + 1) * 4);
     return b;
 }
 
@@ -602,7 +663,8 @@ __device__ inline CcBufs cc_bufs(unsigned char* base, int J, int S, int K, int Q
     b.cctr = reinterpret_cast<float4*>(p);    p += CW * K * 16;
     b.dirty = reinterpret_cast<uint32_t*>(p); p += align16(CW * KW * 4);
     b.gate = reinterpret_cast<uint32_t*>(p);  p += align16(CW * QW * 4);
-    b.hit = reinterpret_cast<uint32_t*>(p);
+    b.hit = reinterpret_cast<uint32_t*>(p);    p += 16;
+    b.bounds = reinterpret_cast<int*>(p);
     b.stats = nullptr;
     return b;
 }
@@ -627,24 +689,73 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         g.sync();
         return 0u;
     }
+    // World work is split into n_parts ranges of the combined obstacle list with
+    // about equal cost, enough parts for roughly two world items per thread; the
+    // range bounds are computed once per chunk.
+    const int n_obs = h.Ns + h.Nc + h.Nb + h.Nh;
+    const int ctot = world_cost(h);
+    const int n_parts =
+        n_obs == 0 ? 0 : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * h.n_sch)), cdiv(n_obs, 4))));
     if (tid == 0) *vhit = 0u;
+    if (n_parts > 0)
+        for (int i = tid; i <= n_parts; i += T) B.bounds[i] = world_index_at(h, (int)((long long)i * ctot / n_parts));
     if (gated) {
         for (int i = tid; i < nw * KW; i += T) B.dirty[i] = 0u;
         for (int i = tid; i < nw * QW; i += T) B.gate[i] = 0u;
     }
-    // A: local joint transforms, one (waypoint, joint) per thread
-    for (int it = tid; it < nw * J; it += T) {
-        const int w = it / J, j = it - w * J;
-        const JointRec& jr = sc.joints[j];
-        joint_local(jr, joint_value(jr, &B.q[w * kDimMax]), &B.pose[(w * J + j) * 12]);
-    }
-    g.sync();
-    // B: chain composition in topological order, one waypoint per thread
-    for (int w = tid; w < nw; w += T) {
-        float* P = &B.pose[w * J * 12];
-        for (int j = 0; j < J; ++j) {
-            const int p = sc.joints[j].idx.x;
-            if (p >= 0 && p < j) compose(&P[p * 12], &P[j * 12], &P[j * 12]);
+    if (J <= 32) {
+        // A+B in registers: a warp segment of SEG lanes per waypoint, lane j
+        // computes joint j's local transform, then pointer jumping composes
+        // the chain -- each round T_j = T_anc(j) o T_j, anc(j) = anc(anc(j)),
+        // ancestors read with shuffles -- in ceil(log2 J) rounds with no
+        // barrier.  Parents precede their children (pack order).
+        const int SEG = J <= 8 ? 8 : (J <= 16 ? 16 : 32);
+        const int per_warp = 32 / SEG, n_warps = T >> 5, warp = tid >> 5, lane = tid & 31;
+        const int sub = lane / SEG, j = lane - sub * SEG;
+        const int rounds = J <= 1 ? 0 : 32 - __clz(J - 1);
+        for (int w0 = warp * per_warp; w0 < nw; w0 += n_warps * per_warp) {
+            const int w = w0 + sub;
+            const bool act = j < J && w < nw;
+            float X[12] = {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f};
+            int a = -1;
+            if (act) {
+                const JointRec& jr = sc.joints[j];
+                joint_local(jr, joint_value(jr, &B.q[w * kDimMax]), X);
+                const int p = jr.idx.x;
+                a = (p >= 0 && p < j) ? p : -1;
+            }
+            for (int r = 0; r < rounds; ++r) {
+                const int src = lane - j + max(a, 0);
+                float Y[12];
+#pragma unroll
+                for (int i = 0; i < 12; ++i) Y[i] = __shfl_sync(0xffffffffu, X[i], src);
+                const int aa = __shfl_sync(0xffffffffu, a, src);
+                if (a >= 0) {
+                    compose(Y, X, X);
+                    a = aa;
+                }
+            }
+            if (act) {
+                float* P = &B.pose[(w * J + j) * 12];
+#pragma unroll
+                for (int i = 0; i < 12; ++i) P[i] = X[i];
+            }
+        }
+    } else {
+        // A: local joint transforms, one (waypoint, joint) per thread
+        for (int it = tid; it < nw * J; it += T) {
+            const int w = it / J, j = it - w * J;
+            const JointRec& jr = sc.joints[j];
+            joint_local(jr, joint_value(jr, &B.q[w * kDimMax]), &B.pose[(w * J + j) * 12]);
+        }
+        g.sync();
+        // B: chain composition in topological order, one waypoint per thread
+        for (int w = tid; w < nw; w += T) {
+            float* P = &B.pose[w * J * 12];
+            for (int j = 0; j < J; ++j) {
+                const int p = sc.joints[j].idx.x;
+                if (p >= 0 && p < j) compose(&P[p * 12], &P[j * 12], &P[j * 12]);
+            }
         }
     }
     g.sync();
@@ -673,11 +784,6 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     }
     g.sync();
     unsigned long long flops = 0;
-    // World work is split into n_parts ranges of the combined obstacle list with
-    // about equal cost, enough parts for roughly two world items per thread.
-    const int n_obs = h.Ns + h.Nc + h.Nb + h.Nh;
-    const int ctot = world_cost(h);
-    const int n_parts = n_obs == 0 ? 0 : max(1, min(cdiv(2 * T, max(1, nw * h.n_sch)), cdiv(n_obs, 4)));
     // D: coarse pre-pass -> dirty groups and touching coarse self pairs
     if (gated) {
         const int n_cw = nw * K * n_parts;
@@ -688,9 +794,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
                 if (B.dirty[w * KW + (k >> 5)] & (1u << (k & 31))) continue;
                 float4 s[1];
                 s[0] = B.cctr[w * K + k];
-                const int j0 = world_index_at(h, (int)((long long)part * ctot / n_parts));
-                const int j1 = world_index_at(h, (int)((long long)(part + 1) * ctot / n_parts));
-                if (obstacles_vs_spheres<1, false>(sc, j0, j1, s, 1, flops))
+                if (obstacles_vs_spheres<1, false>(sc, B.bounds[part], B.bounds[part + 1], s, 1, flops))
                     atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
             } else {
                 const int r = it - n_cw;
@@ -725,8 +829,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
             float4 s[kSphChunk];
 #pragma unroll
             for (int m = 0; m < kSphChunk; ++m) s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : far_sphere();
-            const int j0 = world_index_at(h, (int)((long long)part * ctot / n_parts));
-            const int j1 = world_index_at(h, (int)((long long)(part + 1) * ctot / n_parts));
+            const int j0 = B.bounds[part], j1 = B.bounds[part + 1];
             hit = full_sweep ? obstacles_vs_spheres<kSphChunk, true>(sc, j0, j1, s, ch.y, flops)
                              : obstacles_vs_spheres<kSphChunk, false>(sc, j0, j1, s, ch.y, flops);
         } else if (it >= n_world + n_self) {  // point cloud: (sphere, waypoint)
@@ -749,21 +852,28 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
                 const int na = item.z >> 16, nb = item.z & 0xffff;
                 const float half = 0.5f * inflate;
                 float4 a[kSphChunk];
-                float A[kSphChunk];
+                float thr[kSphChunk], mn[kSphChunk];
 #pragma unroll
                 for (int m = 0; m < kSphChunk; ++m) {
                     a[m] = (m < na) ? C[item.x + m] : far_sphere();
                     a[m].w -= half;
-                    A[m] = sphere_A(a[m]);
+                    thr[m] = -sphere_A(a[m]);
+                    mn[m] = INFINITY;
                 }
+                auto pair_h = [&](float (&v)[kSphChunk], int j) {
+                    float4 b = C[item.y + j];
+                    b.w -= half;
+                    h_sphere<kSphChunk>(v, a, make_float4(-2.0f * b.x, -2.0f * b.y, -2.0f * b.z, -2.0f * b.w),
+                                        sphere_A(b));
+                };
                 int bb = 0;
                 for (; bb < nb; ++bb) {
-                    float4 b = C[item.y + bb];
-                    b.w -= half;
-                    const float4 O = make_float4(-2.0f * b.x, -2.0f * b.y, -2.0f * b.z, -2.0f * b.w);
-                    hit |= min_sphere<kSphChunk>(a, A, O) <= -sphere_A(b);
-                    if (hit && !full_sweep) { ++bb; break; }
+                    float h1[kSphChunk];
+                    pair_h(h1, bb);
+                    fold1(mn, h1);
+                    if (!full_sweep && (bb & 3) == 3 && any_le(mn, thr)) { ++bb; break; }
                 }
+                hit |= any_le(mn, thr);
                 flops += (unsigned long long)bb * na * kFlopPair;
             } else {  // explicit pairs [p0, p0+count) of the pair list (global memory)
                 const int p1 = min(item.x + item.z, h.P);

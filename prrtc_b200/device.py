@@ -46,15 +46,53 @@ def cuda_device(device=None) -> torch.device:
     return d
 
 
+# host->device bytes copied by this module (as_tensor of host data, upload);
+# read and reset by callers that account for their transfers
+H2D_BYTES = [0]
+
+
 def as_tensor(x, dtype: torch.dtype, device: torch.device, cols: int = 0) -> torch.Tensor:
     """Contiguous tensor of `dtype` on `device`; `cols` > 0 reshapes to (-1, cols)."""
     if isinstance(x, torch.Tensor):
+        if x.device != device and device.type == "cuda":
+            H2D_BYTES[0] += x.numel() * torch.empty((), dtype=dtype).element_size()
         t = x.to(device=device, dtype=dtype)
     else:
-        t = torch.as_tensor(np.asarray(x), dtype=dtype).to(device)
+        t = torch.as_tensor(np.asarray(x), dtype=dtype)
+        if device.type == "cuda":
+            H2D_BYTES[0] += t.numel() * t.element_size()
+        t = t.to(device)
     if cols:
         t = t.reshape(-1, cols)
     return t.contiguous()
+
+
+def upload(arrays, device: torch.device) -> list[torch.Tensor]:
+    """Host arrays -> device tensors through ONE pinned staging buffer and one
+    host-to-device copy (each array 256-byte aligned inside it)."""
+    arrays = [np.ascontiguousarray(a) for a in arrays]
+    offs, total = [], 0
+    for a in arrays:
+        offs.append(total)
+        total += (a.nbytes + 255) & ~255
+    total = max(total, 256)
+    host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    hv = host.numpy()
+    for a, o in zip(arrays, offs):
+        hv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+    dev = torch.empty(total, dtype=torch.uint8, device=device)
+    H2D_BYTES[0] += total
+    # torch's caching host allocator records the copy on the stream and keeps
+    # the pinned block out of reuse until that copy has run
+    dev.copy_(host, non_blocking=True)
+    out = []
+    for a, o in zip(arrays, offs):
+        t = dev[o:o + a.nbytes].view(_TORCH_DTYPE[a.dtype.str[1:]]).reshape(a.shape)
+        out.append(t)
+    return out
+
+
+_TORCH_DTYPE = {"f4": torch.float32, "i4": torch.int32, "u1": torch.uint8, "i8": torch.int64, "f8": torch.float64}
 
 
 def ptr(t: torch.Tensor | None) -> int | None:

@@ -34,7 +34,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import REQUIRED_KEYS, DeviceContext, as_tensor, cuda_device, ptr, stream_handle, workspace
+from .device import REQUIRED_KEYS, DeviceContext, as_tensor, cuda_device, ptr, stream_handle, upload, workspace
 
 _COLLISION_MODES = {"binary": 0, "differentiable": 1, "binary_coarse": 2, "binary_coarse_coop": 3}
 PATH_MAX_LEN = 16384
@@ -203,16 +203,18 @@ class _Results:
                     cost = float(torch.linalg.norm(torch.diff(path, dim=0), dim=1).sum())
                     if paths_on_host:
                         path = path.cpu()
-            ta = self.ta[i] if self.ta.dim() == 3 else self.ta
-            tb = self.tb[i] if self.tb.dim() == 3 else self.tb
-            pa = self.pa[i] if self.pa.dim() == 2 else self.pa
-            pb = self.pb[i] if self.pb.dim() == 2 else self.pb
-            na, nb = min(size_a, self.N), min(size_b, self.N)
+            tac = tbc = tap = tbp = None
+            if trees:  # per-problem views only when asked for (each is a tensor op)
+                na, nb = min(size_a, self.N), min(size_b, self.N)
+                batched = self.ta.dim() == 3
+                tac = (self.ta[i] if batched else self.ta)[:, :na]
+                tbc = (self.tb[i] if batched else self.tb)[:, :nb]
+                tap = (self.pa[i] if batched else self.pa)[:na]
+                tbp = (self.pb[i] if batched else self.pb)[:nb]
             out.append(PRRTCResult(
                 solved=solved, path=path, tree_a_size=size_a, tree_b_size=size_b, iterations=int(row[4]),
-                cost=cost, kernel_time_ms=kt,
-                tree_a_configs=ta[:, :na] if trees else None, tree_b_configs=tb[:, :nb] if trees else None,
-                tree_a_parents=pa[:na] if trees else None, tree_b_parents=pb[:nb] if trees else None,
+                cost=cost, kernel_time_ms=kt, tree_a_configs=tac, tree_b_configs=tbc, tree_a_parents=tap,
+                tree_b_parents=tbp,
             ))
         return out
 
@@ -320,12 +322,15 @@ def prrtc_plan(
     return res.to_results()[0]
 
 
-def _pack_worlds(contexts: Sequence[Optional[dict]], B: int):
-    """Padded [B, max_n, feat] world/self tensors + counts (prrtc.py:1009-1067)."""
+def _pack_worlds(contexts: Sequence[Optional[dict]], B: int, skip=()):
+    """Padded [B, max_n, feat] world/self tensors + counts (prrtc.py:1009-1067);
+    keys in `skip` are left out."""
     specs = [("world_spheres", 4, np.float32), ("world_capsules", 7, np.float32), ("world_boxes", 15, np.float32),
              ("world_halfspaces", 6, np.float32), ("self_pairs", 2, np.int32)]
     packed, counts = {}, {}
     for key, feat, dt in specs:
+        if key in skip:
+            continue
         arrs = []
         for i, c in enumerate(contexts):
             if c is None or key not in c or c[key] is None:
@@ -342,6 +347,25 @@ def _pack_worlds(contexts: Sequence[Optional[dict]], B: int):
             p[i, : a.shape[0]] = a
         packed[key], counts[key] = p, n
     return packed, counts
+
+
+def _shared_table(contexts: Sequence[Optional[dict]], key: str):
+    """The table `key` when every context holds the same one (same object or
+    equal contents), else None."""
+    first = contexts[0].get(key) if contexts and contexts[0] is not None else None
+    if first is None:
+        return None
+    a0 = np.asarray(first)
+    for c in contexts[1:]:
+        if c is None:
+            return None
+        x = c.get(key)
+        if x is first:
+            continue
+        if x is None or not np.array_equal(np.asarray(x), a0):
+            return None
+    feat = {"world_spheres": 4, "world_capsules": 7, "world_boxes": 15, "world_halfspaces": 6, "self_pairs": 2}[key]
+    return np.ascontiguousarray(a0, dtype=np.int32 if key == "self_pairs" else np.float32).reshape(-1, feat)
 
 
 def lpt_order(contexts: Sequence[Optional[dict]], goal_counts=None) -> np.ndarray:
@@ -453,16 +477,30 @@ def prrtc_plan_batch(
     bi.min_vals, bi.max_vals = lo.data_ptr(), hi.data_ptr()
     bi.robot = robot_ctx.robot()
     if per_problem and first is not None:
-        packed, counts = _pack_worlds(contexts, B)
-        for key, field in (("world_spheres", "world_spheres"), ("world_capsules", "world_capsules"),
-                           ("world_boxes", "world_boxes"), ("world_halfspaces", "world_halfspaces"),
-                           ("self_pairs", "self_pairs")):
-            t = torch.from_numpy(packed[key]).to(dev)
-            c = torch.from_numpy(counts[key]).to(dev)
-            keep += [t, c]
-            setattr(bi, field, ptr(t))
-            setattr(bi, "max_" + field, int(packed[key].shape[1]))
-            setattr(bi, field + "_count", ptr(c))
+        keys = ("world_spheres", "world_capsules", "world_boxes", "world_halfspaces", "self_pairs")
+        # a table every problem shares (typically the robot's self pairs) goes
+        # once, unbatched, with no count pointer
+        shared = {k: _shared_table(contexts, k) for k in keys}
+        packed, counts = _pack_worlds(contexts, B, skip={k for k in keys if shared[k] is not None})
+        host = []
+        for key in keys:
+            if shared[key] is not None:
+                host.append(shared[key])
+            else:
+                host += [packed[key], counts[key]]
+        dev_t = iter(upload(host, dev))
+        for key in keys:
+            t = next(dev_t)
+            keep.append(t)
+            setattr(bi, key, ptr(t))
+            if shared[key] is not None:
+                setattr(bi, "max_" + key, int(shared[key].shape[0]))
+                setattr(bi, key + "_count", None)
+            else:
+                c = next(dev_t)
+                keep.append(c)
+                setattr(bi, "max_" + key, int(packed[key].shape[1]))
+                setattr(bi, key + "_count", ptr(c))
     elif first is not None:
         w = robot_ctx.world()
         bi.world_spheres, bi.max_world_spheres = w.world_spheres, w.n_world_spheres

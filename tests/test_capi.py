@@ -6,6 +6,7 @@ import ctypes as C
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -93,3 +94,23 @@ def test_api_validation_matches_reference_errors():
         P.prrtc_plan(start, goal, collision_context={"fk_twists": np.zeros((1, 6))})
     with pytest.raises(ValueError, match="single start configuration"):
         P.prrtc_plan(np.zeros((2, 7)), goal, allow_unsafe_no_collision=True)
+
+
+def test_batch_table_sharing_host_logic():
+    """prrtc_plan_batch sends a table once, unbatched, when every problem holds
+    the same one (empty tables included) and pads it per problem otherwise."""
+    from prrtc_b200.prrtc import _pack_worlds, _shared_table
+
+    sp = np.array([[0, 5], [1, 6]], np.int32)
+    ctxs = [{"self_pairs": sp.copy(), "world_spheres": np.zeros((0, 4), np.float32),
+             "world_boxes": np.full((i + 1, 15), i, np.float32)} for i in range(3)]
+    assert np.array_equal(_shared_table(ctxs, "self_pairs"), sp)
+    assert _shared_table(ctxs, "world_spheres").shape == (0, 4)
+    assert _shared_table(ctxs, "world_boxes") is None
+    assert _shared_table(ctxs, "world_capsules") is None  # absent key
+    ctxs[2]["self_pairs"] = sp[:1]
+    assert _shared_table(ctxs, "self_pairs") is None
+    packed, counts = _pack_worlds(ctxs, 3, skip={"world_spheres"})
+    assert "world_spheres" not in packed
+    assert packed["world_boxes"].shape == (3, 3, 15) and counts["world_boxes"].tolist() == [1, 2, 3]
+    assert counts["self_pairs"].tolist() == [2, 2, 1]
