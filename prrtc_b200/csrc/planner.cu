@@ -487,30 +487,44 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
     }
     grp.sync();
     int local_iter = 0;
+    // The per-iteration scalar work runs on warp 0 with one lane per dimension
+    // (Halton digits, extend, connect vector); lane 0 does the rest.  Every lane
+    // repeats lane 0's arithmetic for its own dimension, so results are the
+    // same bits as a sequential loop.
     while (true) {
         ++local_iter;
-        if (tid == 0) {
-            int stop = ld_volatile(P.solved) != 0;
-            if (!stop && local_iter > L.max_iter) {
-                if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
-                atomicMax(P.iter_count, local_iter);
-                stop = 1;
+        if (tid < 32) {
+            const int lane = tid;
+            int stop = 0;
+            if (lane == 0) {
+                stop = ld_volatile(P.solved) != 0;
+                if (!stop && local_iter > L.max_iter) {
+                    if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
+                    atomicMax(P.iter_count, local_iter);
+                    stop = 1;
+                }
             }
+            stop = __shfl_sync(0xffffffffu, stop, 0);
             if (!stop) {
-                halton_sample(X.order, X.halton, dim, L.lo, L.hi, X.sample);
-                const int sa = ld_volatile(&P.sizes[0]), sb = ld_volatile(&P.sizes[1]);
-                const int t = choose_tree(L.balance_mode, local_iter, e % L.E, L.E, sa, sb, L.tree_ratio, X.vamp);
-                X.t = t;
-                X.n_t = min(t == 0 ? sa : sb, N);
+                if (lane < dim) {  // halton_sample, one dimension per lane
+                    const float val = halton_next(X.order[lane & 15], X.halton[lane]);
+                    X.sample[lane] = __fmaf_rn(val, __fsub_rn(L.hi[lane], L.lo[lane]), L.lo[lane]);
+                }
+                if (lane == 0) {
+                    const int sa = ld_volatile(&P.sizes[0]), sb = ld_volatile(&P.sizes[1]);
+                    const int t = choose_tree(L.balance_mode, local_iter, e % L.E, L.E, sa, sb, L.tree_ratio, X.vamp);
+                    X.t = t;
+                    X.n_t = min(t == 0 ? sa : sb, N);
+                }
             }
-            X.stop = stop;
+            if (lane == 0) X.stop = stop;
         }
         grp.sync();
         if (X.stop) break;
         const int t = X.t, o = 1 - t;
         group_nearest(grp, P.tree[t], N, dim, X.n_t, X.sample, X.red_d, X.red_i);
-        if (tid == 0) {
-            if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_t);
+        if (tid < 32) {
+            const int lane = tid;
             const int nn = X.red_i[0];
             int skip = nn == INT_MAX;
             if (!skip) {
@@ -518,17 +532,22 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
                 skip = L.dd && (__ldcg(&P.radii[t][nn]) < nd);
                 if (!skip) {
                     const float scl = nd > 1e-8f ? fminf(1.0f, __fdiv_rn(L.step, nd)) : 1.0f;
-                    for (int d = 0; d < dim; ++d) {
-                        const float bv = __ldcg(&P.tree[t][(size_t)d * N + nn]);
-                        X.base[d] = bv;
-                        X.cand[d] = __fmaf_rn(__fsub_rn(X.sample[d], bv), scl, bv);
-                        X.delta[d] = __fsub_rn(X.cand[d], bv);
+                    if (lane < dim) {
+                        const float bv = __ldcg(&P.tree[t][(size_t)lane * N + nn]);
+                        X.base[lane] = bv;
+                        const float c = __fmaf_rn(__fsub_rn(X.sample[lane], bv), scl, bv);
+                        X.cand[lane] = c;
+                        X.delta[lane] = __fsub_rn(c, bv);
                     }
-                    X.G1 = edge_waypoints(X.delta, dim, L.granularity, L.edge_res);
+                    __syncwarp();
+                    if (lane == 0) X.G1 = edge_waypoints(X.delta, dim, L.granularity, L.edge_res);
                 }
             }
-            X.nn = nn;
-            X.skip = skip;
+            if (lane == 0) {
+                if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_t);
+                X.nn = nn;
+                X.skip = skip;
+            }
         }
         grp.sync();
         if (X.skip) continue;
@@ -558,27 +577,32 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         grp.sync();
         // connect (prrtc_planner.cu:949-1043)
         group_nearest(grp, P.tree[o], N, dim, X.n_o, X.cand, X.red_d, X.red_i);
-        if (tid == 0) {
-            if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_o);
+        if (tid < 32) {
+            const int lane = tid;
             const int cnn = X.red_i[0];
             int n_ext = 0;
             if (cnn != INT_MAX) {
                 const float cd = __fsqrt_rn(X.red_d[0]);
                 if (L.step > 1e-8f && cd > 1e-8f) n_ext = (int)ceilf(__fdiv_rn(cd, L.step));
-                for (int d = 0; d < dim; ++d) {
-                    X.curr[d] = X.cand[d];
-                    X.vec[d] = n_ext > 0 ? __fdiv_rn(__fsub_rn(__ldcg(&P.tree[o][(size_t)d * N + cnn]), X.cand[d]),
-                                                     (float)n_ext)
-                                         : 0.0f;
+                if (lane < dim) {
+                    const float c = X.cand[lane];
+                    X.curr[lane] = c;
+                    X.vec[lane] = n_ext > 0 ? __fdiv_rn(__fsub_rn(__ldcg(&P.tree[o][(size_t)lane * N + cnn]), c),
+                                                        (float)n_ext)
+                                            : 0.0f;
                 }
-                X.G2 = edge_waypoints(X.vec, dim, L.granularity, L.edge_res);
+                __syncwarp();
+                if (lane == 0) X.G2 = edge_waypoints(X.vec, dim, L.granularity, L.edge_res);
             } else {
                 n_ext = -1;
             }
-            X.cnn = cnn;
-            X.n_ext = n_ext;
-            X.ext_parent = X.new_idx;
-            X.abort_ = 0;
+            if (lane == 0) {
+                if (L.stats) atomicAdd(&L.stats[kStatNnNodes], (unsigned long long)X.n_o);
+                X.cnn = cnn;
+                X.n_ext = n_ext;
+                X.ext_parent = X.new_idx;
+                X.abort_ = 0;
+            }
         }
         grp.sync();
         bool failed = X.n_ext < 0;
@@ -586,16 +610,23 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         for (int ext = 0; ext < n_ext && !failed; ++ext) {
             if (X.abort_) { failed = true; break; }
             if (group_edge_collides(grp, sc, B, X.curr, X.vec, dim, X.G2, L.cw)) { failed = true; break; }
-            if (tid == 0) {
-                const int eidx = atomicAdd(&P.sizes[t], 1);
+            if (tid < 32) {
+                const int lane = tid;
+                int eidx = 0;
+                if (lane == 0) eidx = atomicAdd(&P.sizes[t], 1);
+                eidx = __shfl_sync(0xffffffffu, eidx, 0);
                 if (eidx >= N) {
-                    if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
-                    X.ext_idx = -1;
+                    if (lane == 0) {
+                        if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
+                        X.ext_idx = -1;
+                    }
                 } else {
-                    P.par[t][eidx] = X.ext_parent;
-                    X.ext_parent = eidx;
-                    for (int d = 0; d < dim; ++d) X.curr[d] = __fadd_rn(X.curr[d], X.vec[d]);
-                    X.ext_idx = eidx;
+                    if (lane < dim) X.curr[lane] = __fadd_rn(X.curr[lane], X.vec[lane]);
+                    if (lane == 0) {
+                        P.par[t][eidx] = X.ext_parent;
+                        X.ext_parent = eidx;
+                        X.ext_idx = eidx;
+                    }
                 }
             }
             grp.sync();

@@ -177,8 +177,7 @@ cudaError_t launch_nearest(const float* tree, int dim, int N, const int32_t* tre
     constexpr int kQT = 8;
     const bool tiled = batch >= 4 && (N & 3) == 0 && (reinterpret_cast<uintptr_t>(tree) & 15) == 0;
     const int tiles = tiled ? (batch + kQT - 1) / kQT : batch;
-    // 8 CTAs of 256 threads per SM keep enough loads in flight to stream a tree from HBM
-    int splits = std::max(1, (8 * sms + tiles - 1) / tiles);
+    int splits = std::max(1, (4 * sms + tiles - 1) / tiles);
     int slice = (N + splits - 1) / splits;
     slice = std::max(1024, (slice + 1023) & ~1023);
     splits = (N + slice - 1) / slice;

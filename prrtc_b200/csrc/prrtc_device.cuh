@@ -482,7 +482,15 @@ __device__ __forceinline__ void fill(float (&m)[NS], float v) {
     for (int k = 0; k < NS; ++k) m[k] = v;
 }
 
-__device__ __forceinline__ float4 far_sphere() { return make_float4(kFar, kFar, kFar, 0.0f); }
+// An absent sphere (chunk padding, or a sphere whose frame does not exist):
+// NaN centre and radius.  Every test value h is then NaN, which fminf / min.f32
+// skip, or its threshold is NaN, which no comparison passes -- whatever the
+// obstacle's orientation (a far-away finite centre would still fall on the
+// negative side of some halfspaces).
+__device__ __forceinline__ float4 absent_sphere() {
+    const float n = __int_as_float(0x7fc00000);
+    return make_float4(n, n, n, n);
+}
 
 // World obstacles form one list in type order (spheres, capsules, boxes,
 // halfspaces).  Work items take contiguous ranges of that list of roughly equal
@@ -509,7 +517,7 @@ __device__ __forceinline__ int world_index_at(const BlobHeader& h, int x) {
 }
 
 // Obstacles [j0, j1) of the combined list against NS sphere centres held in
-// registers (c.w = radius + inflation; padding spheres sit at kFar).  FULL:
+// registers (c.w = radius + inflation; padding spheres are absent_sphere()).  FULL:
 // test every obstacle; otherwise stop at the first group of kHitCheck
 // obstacles that holds a hit.  flops accumulates the FP32 flops of the tests
 // executed (NS_real real spheres per test).
@@ -519,24 +527,24 @@ constexpr int kHitCheck = 8;
 // sphere; FULL folds two obstacles per three-input minimum, !FULL one obstacle
 // at a time with a hit check every kHitCheck obstacles.  Returns whether some sphere reached its threshold;
 // `done` = obstacles tested.
-template <int NS, bool FULL, class Test>
+template <int NS, bool FULL, bool PAIRS, class Test>
 __device__ __forceinline__ bool sweep_type(float (&m)[NS], const float (&thr)[NS], int lo, int hi, Test test,
                                            int& done) {
     fill(m, INFINITY);
     int o = lo;
-    if constexpr (FULL) {  // throughput form: two obstacles per fold
+    if constexpr (FULL && PAIRS) {  // throughput form: two obstacles per fold
         for (; o + 1 < hi; o += 2) {
             float h1[NS], h2[NS];
             test(h1, o);
             test(h2, o + 1);
             fold2(m, h1, h2);
         }
-    } else {  // early-exit form (inside the planner): fewer live registers
+    } else {  // one obstacle per fold (fewer live registers), early exit unless FULL
         for (; o < hi; ++o) {
             float h1[NS];
             test(h1, o);
             fold1(m, h1);
-            if (((o - lo) & (kHitCheck - 1)) == kHitCheck - 1 && any_le(m, thr)) {
+            if (!FULL && ((o - lo) & (kHitCheck - 1)) == kHitCheck - 1 && any_le(m, thr)) {
                 done = o + 1 - lo;
                 return true;
             }
@@ -551,21 +559,33 @@ __device__ __forceinline__ bool sweep_type(float (&m)[NS], const float (&thr)[NS
     return any_le(m, thr);
 }
 
-template <int NS, bool FULL>
-__device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int j0, int j1, const float4 (&s)[NS],
-                                                     int ns_real, unsigned long long& flops) {
+template <int NS>
+__device__ __forceinline__ uint32_t le_mask(const float (&m)[NS], const float (&thr)[NS]) {
+    uint32_t r = 0u;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) r |= (m[k] <= thr[k] ? 1u : 0u) << k;
+    return r;
+}
+
+// Returns the spheres found in collision as a bit mask (bit k = s[k]).  With
+// !FULL the sweep stops at the first group of obstacles holding a hit, so the
+// mask is then non-zero but may be incomplete.
+template <int NS, bool FULL, bool PAIRS = FULL>
+__device__ __forceinline__ uint32_t obstacles_vs_spheres(const Scene& sc, int j0, int j1, const float4 (&s)[NS],
+                                                         int ns_real, unsigned long long& flops) {
     const BlobHeader& h = *sc.h;
     float m[NS], thr[NS];
-    bool hit = false;
+    uint32_t mask = 0u;
     int done = 0;
     int lo = max(j0, 0), hi = min(j1, h.Ns);
     if (lo < hi) {
 #pragma unroll
         for (int k = 0; k < NS; ++k) thr[k] = -sphere_A(s[k]);
         const float4* ws = sc.ws;
-        hit |= sweep_type<NS, FULL>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_sphere<NS>(v, s, ws[2 * o], ws[2 * o + 1].w); }, done);
+        if (sweep_type<NS, FULL, PAIRS>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_sphere<NS>(v, s, ws[2 * o], ws[2 * o + 1].w); }, done))
+            mask |= le_mask(m, thr);
         flops += (unsigned long long)done * ns_real * kFlopSphere;
-        if (!FULL && hit) return true;
+        if (!FULL && mask) return mask;
     }
     int base = h.Ns;
     lo = max(j0, base) - base;
@@ -573,9 +593,10 @@ __device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int j0, in
     if (lo < hi) {
         fill(thr, 0.0f);
         const float4* wc = sc.wc;
-        hit |= sweep_type<NS, FULL>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_capsule<NS>(v, s, wc[3 * o], wc[3 * o + 1], wc[3 * o + 2]); }, done);
+        if (sweep_type<NS, FULL, PAIRS>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_capsule<NS>(v, s, wc[3 * o], wc[3 * o + 1], wc[3 * o + 2]); }, done))
+            mask |= le_mask(m, thr);
         flops += (unsigned long long)done * ns_real * kFlopCapsule;
-        if (!FULL && hit) return true;
+        if (!FULL && mask) return mask;
     }
     base += h.Nc;
     lo = max(j0, base) - base;
@@ -584,9 +605,10 @@ __device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int j0, in
 #pragma unroll
         for (int k = 0; k < NS; ++k) thr[k] = s[k].w * s[k].w;
         const float4* wb = sc.wb;
-        hit |= sweep_type<NS, FULL>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_box<NS>(v, s, wb[4 * o], wb[4 * o + 1], wb[4 * o + 2], wb[4 * o + 3]); }, done);
+        if (sweep_type<NS, FULL, PAIRS>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_box<NS>(v, s, wb[4 * o], wb[4 * o + 1], wb[4 * o + 2], wb[4 * o + 3]); }, done))
+            mask |= le_mask(m, thr);
         flops += (unsigned long long)done * ns_real * kFlopBox;
-        if (!FULL && hit) return true;
+        if (!FULL && mask) return mask;
     }
     base += h.Nb;
     lo = max(j0, base) - base;
@@ -595,10 +617,11 @@ __device__ __forceinline__ bool obstacles_vs_spheres(const Scene& sc, int j0, in
 #pragma unroll
         for (int k = 0; k < NS; ++k) thr[k] = s[k].w;
         const float4* wh = sc.wh;
-        hit |= sweep_type<NS, true>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_halfspace<NS>(v, s, wh[o]); }, done);
+        if (sweep_type<NS, true, false>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_halfspace<NS>(v, s, wh[o]); }, done))
+            mask |= le_mask(m, thr);
         flops += (unsigned long long)done * ns_real * kFlopHalfspace;
     }
-    return hit;
+    return mask;
 }
 
 // ----------------------------------------------------------------------------- thread groups
@@ -631,7 +654,7 @@ struct CcBufs {
     uint32_t* dirty; // [CW][KW]
     uint32_t* gate;  // [CW][QW]
     uint32_t* hit;   // [1]
-    int* bounds;     // [kMaxParts + 1] first obstacle of each world part
+    int* bounds;     // [2][kMaxParts + 1] first obstacle of each world part (fine pass, coarse pass)
     unsigned long long* stats;  // optional device counters (kStat*), may be null
 };
 
@@ -648,7 +671,7 @@ __host__ __device__ inline int cc_smem_bytes(int J, int S, int K, int Q, int CW)
     b += align16(CW * KW * 4);
     b += align16(CW * QW * 4);
     b += 16;
-    b += align16((kMaxParts + 1) * 4);
+    b += align16(2 * (kMaxParts + 1) * 4);
     return b;
 }
 
@@ -667,6 +690,26 @@ __device__ inline CcBufs cc_bufs(unsigned char* base, int J, int S, int K, int Q
     b.bounds = reinterpret_cast<int*>(p);
     b.stats = nullptr;
     return b;
+}
+
+// Sphere centres of waypoint w (fine, and coarse when gated) from its frames in
+// B.pose: spheres first, first + step, ... of this caller.
+__device__ __forceinline__ void cc_centres(const Scene& sc, const CcBufs& B, int w, int first, int step, int J, int S,
+                                           int S_pad, int K, bool gated, float inflate) {
+    for (int s = first; s < S; s += step) {
+        const int f = sc.sfr[s];
+        float4 l = sc.sph[s];
+        l.w += inflate;
+        B.ctr[w * S_pad + s] = f >= 0 ? xform_point(&B.pose[(w * J + f) * 12], l) : absent_sphere();
+    }
+    if (gated) {
+        for (int k = first; k < K; k += step) {
+            float4 l = sc.grp[2 * k];
+            l.w += inflate;
+            const int f = __float_as_int(sc.grp[2 * k + 1].x);
+            B.cctr[w * K + k] = f >= 0 ? xform_point(&B.pose[(w * J + f) * 12], l) : absent_sphere();
+        }
+    }
 }
 
 // Collision check of nw (<= CW <= 32) configurations already in B.q.  Every
@@ -696,9 +739,17 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     const int ctot = world_cost(h);
     const int n_parts =
         n_obs == 0 ? 0 : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * h.n_sch)), cdiv(n_obs, 4))));
+    // coarse pass: one item = up to 8 coarse spheres of a waypoint over a part
+    const int KC = cdiv(K, 8);
+    const int n_parts_c =
+        (n_obs == 0 || !gated) ? 0 : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * KC)), cdiv(n_obs, 4))));
+    int* bounds_c = B.bounds + (kMaxParts + 1);
     if (tid == 0) *vhit = 0u;
     if (n_parts > 0)
         for (int i = tid; i <= n_parts; i += T) B.bounds[i] = world_index_at(h, (int)((long long)i * ctot / n_parts));
+    if (n_parts_c > 0)
+        for (int i = tid; i <= n_parts_c; i += T)
+            bounds_c[i] = world_index_at(h, (int)((long long)i * ctot / n_parts_c));
     if (gated) {
         for (int i = tid; i < nw * KW; i += T) B.dirty[i] = 0u;
         for (int i = tid; i < nw * QW; i += T) B.gate[i] = 0u;
@@ -740,6 +791,10 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
 #pragma unroll
                 for (int i = 0; i < 12; ++i) P[i] = X[i];
             }
+            __syncwarp();
+            // C, fused: the segment that composed waypoint w's frames places its
+            // sphere centres (warp-local data, so no CTA barrier in between)
+            if (w < nw) cc_centres(sc, B, w, j, SEG, J, S, S_pad, K, gated, inflate);
         }
     } else {
         // A: local joint transforms, one (waypoint, joint) per thread
@@ -757,45 +812,28 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
                 if (p >= 0 && p < j) compose(&P[p * 12], &P[j * 12], &P[j * 12]);
             }
         }
+        g.sync();
+        // C: sphere centres, one (waypoint, sphere) per thread
+        for (int it = tid; it < nw * T; it += T) cc_centres(sc, B, it / T, it % T, T, J, S, S_pad, K, gated, inflate);
     }
     g.sync();
-    // C: sphere centres (fine, and coarse when gated)
-    for (int it = tid; it < nw * S; it += T) {
-        const int w = it / S, s = it - w * S;
-        const int f = sc.sfr[s];
-        float4 l = sc.sph[s];
-        l.w += inflate;
-        float4 c;
-        if (f >= 0) c = xform_point(&B.pose[(w * J + f) * 12], l);
-        else c = make_float4(kFar, kFar, kFar, l.w);
-        B.ctr[w * S_pad + s] = c;
-    }
-    if (gated) {
-        for (int it = tid; it < nw * K; it += T) {
-            const int w = it / K, k = it - w * K;
-            float4 l = sc.grp[2 * k];
-            l.w += inflate;
-            const int f = __float_as_int(sc.grp[2 * k + 1].x);
-            float4 c;
-            if (f >= 0) c = xform_point(&B.pose[(w * J + f) * 12], l);
-            else c = make_float4(kFar, kFar, kFar, l.w);
-            B.cctr[w * K + k] = c;
-        }
-    }
     g.sync();
     unsigned long long flops = 0;
     // D: coarse pre-pass -> dirty groups and touching coarse self pairs
     if (gated) {
-        const int n_cw = nw * K * n_parts;
+        const int n_cw = nw * KC * n_parts_c;
         for (int it = tid; it < n_cw + nw * Q; it += T) {
             if (it < n_cw) {
-                const int part = it / (nw * K), r = it - part * (nw * K);
-                const int k = r / nw, w = r - k * nw;
-                if (B.dirty[w * KW + (k >> 5)] & (1u << (k & 31))) continue;
-                float4 s[1];
-                s[0] = B.cctr[w * K + k];
-                if (obstacles_vs_spheres<1, false>(sc, B.bounds[part], B.bounds[part + 1], s, 1, flops))
-                    atomicOr(&B.dirty[w * KW + (k >> 5)], 1u << (k & 31));
+                const int part = it / (nw * KC), r = it - part * (nw * KC);
+                const int kc = r / nw, w = r - kc * nw;
+                const int k0 = kc * 8, nk = min(8, K - k0);
+                float4 s[8];
+#pragma unroll
+                for (int m = 0; m < 8; ++m) s[m] = m < nk ? B.cctr[w * K + k0 + m] : absent_sphere();
+                const uint32_t hitk =
+                    obstacles_vs_spheres<8, true, false>(sc, bounds_c[part], bounds_c[part + 1], s, nk, flops);
+                // 8 | 32: a chunk's bits never straddle two words
+                if (hitk) atomicOr(&B.dirty[w * KW + (k0 >> 5)], hitk << (k0 & 31));
             } else {
                 const int r = it - n_cw;
                 const int qq = r / nw, w = r - qq * nw;
@@ -828,10 +866,10 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
             if (gated && ch.z >= 0 && !(B.dirty[w * KW + (ch.z >> 5)] & (1u << (ch.z & 31)))) continue;
             float4 s[kSphChunk];
 #pragma unroll
-            for (int m = 0; m < kSphChunk; ++m) s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : far_sphere();
+            for (int m = 0; m < kSphChunk; ++m) s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : absent_sphere();
             const int j0 = B.bounds[part], j1 = B.bounds[part + 1];
-            hit = full_sweep ? obstacles_vs_spheres<kSphChunk, true>(sc, j0, j1, s, ch.y, flops)
-                             : obstacles_vs_spheres<kSphChunk, false>(sc, j0, j1, s, ch.y, flops);
+            hit = (full_sweep ? obstacles_vs_spheres<kSphChunk, true>(sc, j0, j1, s, ch.y, flops)
+                              : obstacles_vs_spheres<kSphChunk, false>(sc, j0, j1, s, ch.y, flops)) != 0u;
         } else if (it >= n_world + n_self) {  // point cloud: (sphere, waypoint)
             const int r = it - n_world - n_self;
             const int si = r / nw;
@@ -855,7 +893,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
                 float thr[kSphChunk], mn[kSphChunk];
 #pragma unroll
                 for (int m = 0; m < kSphChunk; ++m) {
-                    a[m] = (m < na) ? C[item.x + m] : far_sphere();
+                    a[m] = (m < na) ? C[item.x + m] : absent_sphere();
                     a[m].w -= half;
                     thr[m] = -sphere_A(a[m]);
                     mn[m] = INFINITY;

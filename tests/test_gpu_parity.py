@@ -374,3 +374,29 @@ def test_legacy_iteration_matches_oracle(cuda, orc, N, batch):
         assert valid[b].item() == int(slot < N) and par[b].item() == 0
         if slot < N:
             assert np.array_equal(out[t][:, slot].view(np.int32), cfg[b]) and outp[t][slot] == 0
+
+
+@pytest.mark.parametrize("mode", [0, 3])
+def test_absent_spheres_and_downward_halfspace(cuda, orc, mode):
+    """A sphere on a link that does not exist and chunk padding (57 spheres) must
+    never collide, even with a halfspace whose normal points down (a ceiling):
+    the padding must not sit at a finite far-away point."""
+    from prrtc_b200.collision import CollisionChecker
+
+    pr = make_problem("tabletop", 6)
+    ctx = dict(pr.context)
+    ctx["world_halfspaces"] = np.concatenate(
+        [ctx["world_halfspaces"], np.array([[0, 0, -1, 0, 0, 2.5]], np.float32)])
+    J = ctx["fk_parent_idx"].shape[0]
+    ctx["sphere_link_idx"] = np.concatenate([ctx["sphere_link_idx"], np.array([J + 5], np.int32)])
+    ctx["sphere_local"] = np.concatenate([ctx["sphere_local"], np.zeros((1, 3), np.float32)])
+    ctx["sphere_radius"] = np.concatenate([ctx["sphere_radius"], np.array([0.05], np.float32)])
+    rng = np.random.default_rng(23)
+    q = rng.uniform(pr.lower, pr.upper, (2000, pr.dim)).astype(np.float32)
+    names = ["binary", "differentiable", "binary_coarse", "binary_coarse_coop"]
+    mine = CollisionChecker(ctx, pr.dim, names[mode], 0.02).check(q).cpu().numpy()
+    sc = orc.Scene(ctx, pr.dim)
+    ora = sc.check_configs(q, mode, 0.02)
+    far = np.abs(sc.min_distances(q)) > 1e-4
+    assert np.array_equal(mine[far], ora[far])
+    assert 0.02 < mine.mean() < 0.98
