@@ -388,7 +388,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
     from prrtc_b200 import _lib as L
     from prrtc_b200.batch import STAT_CONFIGS, STAT_EDGES, STAT_FLOPS, STAT_NN_NODES, BatchPlanner, PlanSettings
     from prrtc_b200.collision import CollisionChecker
-    from prrtc_b200.prrtc import prrtc_nearest_neighbor, prrtc_plan_batch
+    from prrtc_b200.prrtc import prrtc_nearest_neighbor, prrtc_plan_batch, prrtc_plan_batch_async
 
     out = {}
     peaks = measured_peaks()
@@ -437,22 +437,34 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
         host_in[N] = (np.stack([p.start for p in ps]), goals, [p.context for p in ps],
                       [p.goals.shape[0] for p in ps])
 
+    e2e_streams = {N: torch.cuda.Stream(device=dev) for N in planners}
+
     def e2e_step():
+        # every bucket queued on its own stream first, then the results read
+        # back: the host prepares bucket k+1 while bucket k runs
         solved, d2h = 0, 0
+        pending = {}
+        main = torch.cuda.current_stream()
         for N, pl in planners.items():
             ps = pl.problems
             starts, goals, ctxs, gcounts = host_in[N]
-            res = prrtc_plan_batch(starts, goals, max_iterations=settings.max_iterations,
-                                   num_new_samples=tuned[N]["num_new_samples"],
-                                   waypoint_chunk=tuned[N]["waypoint_chunk"],
-                                   max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper,
-                                   collision_context=ctxs, collision_checker=settings.collision_checker,
-                                   goal_counts=gcounts, edge_resolution=settings.edge_resolution,
-                                   threads_per_explorer=tuned[N]["threads_per_explorer"], return_trees=False,
-                                   paths_on_host=True)
+            e2e_streams[N].wait_stream(main)
+            with torch.cuda.stream(e2e_streams[N]):
+                pending[N] = prrtc_plan_batch_async(
+                    starts, goals, max_iterations=settings.max_iterations,
+                    num_new_samples=tuned[N]["num_new_samples"], waypoint_chunk=tuned[N]["waypoint_chunk"],
+                    max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper, collision_context=ctxs,
+                    collision_checker=settings.collision_checker, goal_counts=gcounts,
+                    edge_resolution=settings.edge_resolution,
+                    threads_per_explorer=tuned[N]["threads_per_explorer"], return_trees=False, paths_on_host=True)
+        for N, pl in planners.items():
+            ps = pl.problems
+            res = pending[N].results()
             solved += sum(r.solved for r in res)
             lmax = max((r.path.shape[0] for r in res if r.solved), default=0)
             d2h += len(ps) * 16 * 4 + len(ps) * lmax * ps[0].dim * 4
+        for st in e2e_streams.values():
+            main.wait_stream(st)
         return solved, d2h
 
     e2e_step()  # warm: first-call allocations
@@ -469,8 +481,9 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
     dt = time.perf_counter() - t0
     out["e2e"] = {"value": solved / dt, "unit": "plans/s", "h2d_bytes_per_step": _device.H2D_BYTES[0] // k_e2e,
                   "d2h_bytes_per_step": d2h // k_e2e, "steps": k_e2e,
-                  "api": "prrtc_b200.prrtc_plan_batch (per-problem collision_context dicts, host numpy inputs, "
-                         "one call per capacity bucket, paths copied to the host)"}
+                  "api": "prrtc_b200.prrtc_plan_batch_async + .results() (per-problem collision_context dicts, "
+                         "host numpy inputs, one call per capacity bucket on its own stream, paths copied to "
+                         "the host)"}
 
     # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
     torch.cuda.synchronize()

@@ -11,6 +11,7 @@ from .prrtc import (  # noqa: F401
     prrtc_nearest_neighbor,
     prrtc_plan,
     prrtc_plan_batch,
+    prrtc_plan_batch_async,
 )
 from .pointcloud import PointCloud, PointCloudChecker, prrtc_plan_robogpu  # noqa: E402,F401
 
@@ -18,6 +19,7 @@ __all__ = [
     "PRRTCResult",
     "prrtc_plan",
     "prrtc_plan_batch",
+    "prrtc_plan_batch_async",
     "prrtc_nearest_neighbor",
     "prrtc_extend",
     "prrtc_iteration",

@@ -187,13 +187,17 @@ class _Results:
             lmax = int(max(0, host[:, 10].max())) if self.B else 0
             hpaths = self.paths[:, :lmax].cpu().numpy() if lmax > 0 else None
         out = []
+        # plain Python scalars for the per-problem loop (numpy scalar access is slow)
+        rows = host.tolist()
+        kts = host[:, 9].copy().view(np.float32).tolist()
+        costs = host[:, 11].copy().view(np.float32).tolist()
         for i in range(self.B):
-            row = host[i]
-            solved = bool(row[8] == 1)
-            size_a, size_b = int(row[0]), int(row[1])
-            length = int(row[10])
-            kt = float(row[9:10].view(np.float32)[0])
-            cost = float(row[11:12].view(np.float32)[0]) if solved else float("inf")
+            row = rows[i]
+            solved = row[8] == 1
+            size_a, size_b = row[0], row[1]
+            length = row[10]
+            kt = kts[i]
+            cost = costs[i] if solved else float("inf")
             path = None
             if solved:
                 if length > 0:
@@ -212,7 +216,7 @@ class _Results:
                 tap = (self.pa[i] if batched else self.pa)[:na]
                 tbp = (self.pb[i] if batched else self.pb)[:nb]
             out.append(PRRTCResult(
-                solved=solved, path=path, tree_a_size=size_a, tree_b_size=size_b, iterations=int(row[4]),
+                solved=solved, path=path, tree_a_size=size_a, tree_b_size=size_b, iterations=row[4],
                 cost=cost, kernel_time_ms=kt, tree_a_configs=tac, tree_b_configs=tbc, tree_a_parents=tap,
                 tree_b_parents=tbp,
             ))
@@ -322,29 +326,45 @@ def prrtc_plan(
     return res.to_results()[0]
 
 
+_TABLES = (("world_spheres", 4, np.float32), ("world_capsules", 7, np.float32), ("world_boxes", 15, np.float32),
+           ("world_halfspaces", 6, np.float32), ("self_pairs", 2, np.int32))
+_FEAT = {k: f for k, f, _ in _TABLES}
+
+
+def _tables(contexts: Sequence[Optional[dict]], key: str, feat: int, dt) -> list:
+    """Table `key` of every context as a 2-D array (absent = zero rows)."""
+    out = []
+    empty = np.zeros((0, feat), dtype=dt)
+    for i, c in enumerate(contexts):
+        x = None if c is None else c.get(key)
+        if x is None:
+            out.append(empty)
+            continue
+        a = x if (isinstance(x, np.ndarray) and x.dtype == dt) else np.asarray(x, dtype=dt)
+        if a.ndim != 2 or a.shape[1] != feat:
+            raise ValueError(f"collision_context[{i}]['{key}'] must have shape (N, {feat}), got {a.shape}")
+        out.append(a)
+    return out
+
+
 def _pack_worlds(contexts: Sequence[Optional[dict]], B: int, skip=()):
     """Padded [B, max_n, feat] world/self tensors + counts (prrtc.py:1009-1067);
     keys in `skip` are left out."""
-    specs = [("world_spheres", 4, np.float32), ("world_capsules", 7, np.float32), ("world_boxes", 15, np.float32),
-             ("world_halfspaces", 6, np.float32), ("self_pairs", 2, np.int32)]
     packed, counts = {}, {}
-    for key, feat, dt in specs:
+    for key, feat, dt in _TABLES:
         if key in skip:
             continue
-        arrs = []
-        for i, c in enumerate(contexts):
-            if c is None or key not in c or c[key] is None:
-                a = np.zeros((0, feat), dtype=dt)
-            else:
-                a = np.asarray(c[key], dtype=dt)
-                if a.ndim != 2 or a.shape[1] != feat:
-                    raise ValueError(f"collision_context[{i}]['{key}'] must have shape (N, {feat}), got {a.shape}")
-            arrs.append(a)
-        n = np.array([a.shape[0] for a in arrs], dtype=np.int32)
+        arrs = _tables(contexts, key, feat, dt)
+        n = np.fromiter((a.shape[0] for a in arrs), dtype=np.int32, count=len(arrs))
         m = int(n.max()) if B else 0
         p = np.zeros((B, m, feat), dtype=dt)
-        for i, a in enumerate(arrs):
-            p[i, : a.shape[0]] = a
+        total = int(n.sum())
+        if total:
+            # one scatter: row r of the concatenation goes to (problem, row within problem)
+            flat = np.concatenate(arrs, axis=0)
+            prob = np.repeat(np.arange(B), n)
+            within = np.arange(total) - np.repeat(np.cumsum(n) - n, n)
+            p[prob, within] = flat
         packed[key], counts[key] = p, n
     return packed, counts
 
@@ -356,33 +376,40 @@ def _shared_table(contexts: Sequence[Optional[dict]], key: str):
     if first is None:
         return None
     a0 = np.asarray(first)
+    b0 = None
     for c in contexts[1:]:
         if c is None:
             return None
         x = c.get(key)
         if x is first:
             continue
-        if x is None or not np.array_equal(np.asarray(x), a0):
+        if x is None:
             return None
-    feat = {"world_spheres": 4, "world_capsules": 7, "world_boxes": 15, "world_halfspaces": 6, "self_pairs": 2}[key]
-    return np.ascontiguousarray(a0, dtype=np.int32 if key == "self_pairs" else np.float32).reshape(-1, feat)
+        x = np.asarray(x)
+        if x.shape != a0.shape:
+            return None
+        if x.size == 0:
+            continue
+        if b0 is None:
+            b0 = a0.tobytes()
+        if x.tobytes() != b0:
+            return None
+    return np.ascontiguousarray(a0, dtype=np.int32 if key == "self_pairs" else np.float32).reshape(-1, _FEAT[key])
+
+
+_LPT_WEIGHTS = (("world_spheres", 1.0), ("world_capsules", 2.0), ("world_boxes", 3.0), ("world_halfspaces", 1.0))
 
 
 def lpt_order(contexts: Sequence[Optional[dict]], goal_counts=None) -> np.ndarray:
     """Longest-processing-time order: problems with the most collision work first."""
-    cost = []
-    for c in contexts:
-        if c is None:
-            cost.append(0.0)
-            continue
-        ns = sum(int(np.asarray(c.get(k, np.zeros((0,)))).shape[0]) * w
-                 for k, w in (("world_spheres", 1.0), ("world_capsules", 2.0), ("world_boxes", 3.0),
-                              ("world_halfspaces", 1.0)))
-        cost.append(ns)
-    return np.argsort(-np.asarray(cost), kind="stable").astype(np.int32)
+    cost = np.zeros(len(contexts), dtype=np.float64)
+    for k, w in _LPT_WEIGHTS:
+        cost += w * np.fromiter(((0 if c is None or c.get(k) is None else len(c[k])) for c in contexts),
+                                dtype=np.float64, count=len(contexts))
+    return np.argsort(-cost, kind="stable").astype(np.int32)
 
 
-def prrtc_plan_batch(
+def prrtc_plan_batch_async(
     start_configs,
     goal_configs,
     max_iterations: int = 1_000_000,
@@ -417,8 +444,11 @@ def prrtc_plan_batch(
     r_env: float = 0.02,
     tail_explorers: bool = True,
     device=None,
-) -> list[PRRTCResult]:
-    """Plan B independent problems (prrtc.py:882-1434).
+) -> "PendingBatch":
+    """Plan B independent problems (prrtc.py:882-1434), without waiting: the
+    work is queued on the current stream and ``.results()`` of the returned
+    handle reads it back.  Several batches (for example one per tree-capacity
+    bucket, each on its own stream) can be in flight at once.
 
     ``collision_context`` is one dict shared by every problem, or a list/tuple of
     per-problem dicts (robot tables from the first non-None entry; worlds and
@@ -546,7 +576,29 @@ def prrtc_plan_batch(
     else:
         raise ValueError(f"launch must be 'persistent' or 'per_problem', got {launch!r}")
     res.extract(sp)
-    return res.to_results(trees=return_trees, paths_on_host=paths_on_host)
+    # everything the queued kernels read stays referenced until results()
+    keep += [starts, goals, lo, hi, robot_ctx] + ([ws] if launch == "persistent" else [])
+    return PendingBatch(res, keep, torch.cuda.current_stream(dev), return_trees, paths_on_host)
+
+
+class PendingBatch:
+    """A queued batch: its outputs plus every input it still reads."""
+
+    def __init__(self, res: "_Results", keep: list, stream, trees: bool, paths_on_host: bool):
+        self.res, self.keep, self.stream = res, keep, stream
+        self.trees, self.paths_on_host = trees, paths_on_host
+
+    def results(self) -> list[PRRTCResult]:
+        with torch.cuda.stream(self.stream):
+            out = self.res.to_results(trees=self.trees, paths_on_host=self.paths_on_host)
+        self.keep = []
+        return out
+
+
+def prrtc_plan_batch(start_configs, goal_configs, *args, **kwargs) -> list[PRRTCResult]:
+    """Plan B independent problems (prrtc.py:882-1434): the arguments of
+    ``prrtc_plan_batch_async``, waiting for the results."""
+    return prrtc_plan_batch_async(start_configs, goal_configs, *args, **kwargs).results()
 
 
 def _plan_per_problem(lib, bi, res, attrs, tun, contexts, robot_ctx, starts, goals, goal_counts, lo, hi, dev,

@@ -400,3 +400,32 @@ def test_absent_spheres_and_downward_halfspace(cuda, orc, mode):
     far = np.abs(sc.min_distances(q)) > 1e-4
     assert np.array_equal(mine[far], ora[far])
     assert 0.02 < mine.mean() < 0.98
+
+
+def test_async_batches_on_two_streams(cuda, orc):
+    """Two batches of different tree capacity queued on two streams before
+    either is read back; both read back solved, re-validating paths."""
+    from prrtc_b200 import prrtc_plan_batch_async
+
+    groups = {4096: [make_problem("uneven", 400 + i) for i in range(4)],
+              16384: [make_problem("uneven", 410 + i) for i in range(4)]}
+    streams = {N: torch.cuda.Stream(device=cuda) for N in groups}
+    pending = {}
+    for N, probs in groups.items():
+        G = max(p.goals.shape[0] for p in probs)
+        goals = np.zeros((len(probs), G, probs[0].dim), np.float32)
+        for i, p in enumerate(probs):
+            goals[i, : p.goals.shape[0]] = p.goals
+        with torch.cuda.stream(streams[N]):
+            pending[N] = prrtc_plan_batch_async(
+                np.stack([p.start for p in probs]), goals, max_iterations=5000, num_new_samples=8, max_nodes=N,
+                min_vals=probs[0].lower, max_vals=probs[0].upper, collision_context=[p.context for p in probs],
+                collision_checker="binary_coarse_coop", goal_counts=[p.goals.shape[0] for p in probs],
+                edge_resolution=0.01, return_trees=False, paths_on_host=True)
+    for N, probs in groups.items():
+        res = pending[N].results()
+        assert sum(r.solved for r in res) >= len(probs) - 1
+        for p, r in zip(probs, res):
+            if r.solved:
+                ok, md = orc.Scene(p.context, p.dim).validate_path(r.path.numpy(), 0.01)
+                assert ok, md
