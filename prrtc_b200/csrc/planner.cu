@@ -903,10 +903,10 @@ cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
         long long grid = (long long)per_sm * device_sm_count();
         if (L.resident > 0) grid = std::min<long long>(grid, L.resident);
         const long long work = warps ? (long long)L.B * ((L.E + kWarpsPerCta - 1) / kWarpsPerCta) : (long long)L.B * L.E;
-        // without tail join a CTA beyond the slot count would find no work; with
-        // it, every resident CTA is useful until the last problem ends (and CTAs
-        // queued behind another launch join this one's stragglers when they start)
-        if (!L.tail_join) grid = std::min<long long>(grid, work);
+        // no more CTAs than explorer slots: with several batches in flight (one per
+        // capacity bucket) a full-GPU grid per launch measured slower, its CTAs
+        // piling extra explorers onto a few problems
+        grid = std::min<long long>(grid, work);
         kern<<<(unsigned)std::max<long long>(grid, 1), threads, dyn, st>>>(L);
     } else {
         explore_kernel<<<dim3(L.E, L.B), L.threads, dyn, st>>>(L);
