@@ -449,22 +449,16 @@ __device__ int choose_tree(int mode, int local_iter, int bid, int nblocks, int s
 // waypoints c, c+nchunk, c+2*nchunk, ... -- so the first pass already samples
 // the whole edge and a colliding edge usually stops after one pass.  The
 // verdict (any waypoint in collision) does not depend on the order.
+// The waypoints are computed inside the checker's FK step (no staging pass).
 template <class Grp>
 __device__ bool group_edge_collides(const Grp& grp, const Scene& sc, const CcBufs& B, const float* base,
-                                    const float* delta, int dim, int G, int CW) {
-    const int tid = grp.rank(), T = grp.size();
-    if (B.stats && tid == 0) atomicAdd(&B.stats[kStatEdges], 1ull);
+                                    const float* delta, int G, int CW, int& par) {
+    if (B.stats && grp.rank() == 0) atomicAdd(&B.stats[kStatEdges], 1ull);
     const int nchunk = (G + CW - 1) / CW;
     for (int c = 0; c < nchunk; ++c) {
         const int nw = (G - c + nchunk - 1) / nchunk;  // waypoints c, c+nchunk, ... below G
-        for (int i = tid; i < nw * dim; i += T) {
-            const int w = i / dim, d = i - w * dim;
-            const int k = c + w * nchunk;
-            const float t = __fdiv_rn((float)(k + 1), (float)G);
-            B.q[w * kDimMax + d] = __fmaf_rn(t, delta[d], base[d]);
-        }
-        grp.sync();
-        if (cc_chunk(grp, sc, B, nw, true, false) != 0u) return true;
+        const EdgeSrc e{base, delta, G, nchunk, c};
+        if (cc_chunk(grp, sc, B, nw, true, false, par, &e) != 0u) return true;
     }
     return false;
 }
@@ -484,8 +478,10 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         prime_order(e, X.order);
         for (int d = 0; d < kDimMax; ++d) X.halton[d] = 1;
         X.vamp = 0;
+        B.hit[0] = B.hit[1] = 0u;  // the checker's two result words
     }
     grp.sync();
+    int par = 0;  // which hit word the next checker call uses (same in every thread)
     int local_iter = 0;
     // The per-iteration scalar work runs on warp 0 with one lane per dimension
     // (Halton digits, extend, connect vector); lane 0 does the rest.  Every lane
@@ -495,9 +491,13 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         ++local_iter;
         if (tid < 32) {
             const int lane = tid;
-            int stop = 0;
+            int stop = 0, sa = 0, sb = 0;
             if (lane == 0) {
-                stop = ld_volatile(P.solved) != 0;
+                // the three loads go out together: one round trip, not three
+                const int sv = ld_volatile(P.solved);
+                sa = ld_volatile(&P.sizes[0]);
+                sb = ld_volatile(&P.sizes[1]);
+                stop = sv != 0;
                 if (!stop && local_iter > L.max_iter) {
                     if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
                     atomicMax(P.iter_count, local_iter);
@@ -511,7 +511,6 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
                     X.sample[lane] = __fmaf_rn(val, __fsub_rn(L.hi[lane], L.lo[lane]), L.lo[lane]);
                 }
                 if (lane == 0) {
-                    const int sa = ld_volatile(&P.sizes[0]), sb = ld_volatile(&P.sizes[1]);
                     const int t = choose_tree(L.balance_mode, local_iter, e % L.E, L.E, sa, sb, L.tree_ratio, X.vamp);
                     X.t = t;
                     X.n_t = min(t == 0 ? sa : sb, N);
@@ -528,12 +527,14 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
             const int nn = X.red_i[0];
             int skip = nn == INT_MAX;
             if (!skip) {
+                // radius and node loads issued together (one round trip)
+                const float rad = L.dd ? __ldcg(&P.radii[t][nn]) : 0.0f;
+                const float bv = lane < dim ? __ldcg(&P.tree[t][(size_t)lane * N + nn]) : 0.0f;
                 const float nd = __fsqrt_rn(X.red_d[0]);
-                skip = L.dd && (__ldcg(&P.radii[t][nn]) < nd);
+                skip = L.dd && (rad < nd);
                 if (!skip) {
                     const float scl = nd > 1e-8f ? fminf(1.0f, __fdiv_rn(L.step, nd)) : 1.0f;
                     if (lane < dim) {
-                        const float bv = __ldcg(&P.tree[t][(size_t)lane * N + nn]);
                         X.base[lane] = bv;
                         const float c = __fmaf_rn(__fsub_rn(X.sample[lane], bv), scl, bv);
                         X.cand[lane] = c;
@@ -551,7 +552,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         }
         grp.sync();
         if (X.skip) continue;
-        if (group_edge_collides(grp, sc, B, X.base, X.delta, dim, X.G1, L.cw)) {
+        if (group_edge_collides(grp, sc, B, X.base, X.delta, X.G1, L.cw, par)) {
             if (tid == 0 && L.dd) radius_shrink(P.radii[t], X.nn, L.dd_alpha, L.dd_radius, L.dd_min_radius);
             continue;
         }
@@ -609,7 +610,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         const int n_ext = X.n_ext;
         for (int ext = 0; ext < n_ext && !failed; ++ext) {
             if (X.abort_) { failed = true; break; }
-            if (group_edge_collides(grp, sc, B, X.curr, X.vec, dim, X.G2, L.cw)) { failed = true; break; }
+            if (group_edge_collides(grp, sc, B, X.curr, X.vec, X.G2, L.cw, par)) { failed = true; break; }
             if (tid < 32) {
                 const int lane = tid;
                 int eidx = 0;

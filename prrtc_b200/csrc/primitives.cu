@@ -349,6 +349,9 @@ __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const
     }
     sc.pairs = reinterpret_cast<const int2*>(pairs);
     sc.pc = pc;
+    if (tid == 0) B.hit[0] = B.hit[1] = 0u;
+    int par = 0;
+    __syncthreads();
     for (int c0 = blockIdx.x * CW; c0 < n; c0 += gridDim.x * CW) {
         const int nw = min(CW, n - c0);
         for (int i = tid; i < nw * dim; i += blockDim.x) {
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const
             B.q[w * kDimMax + d] = configs[(size_t)(c0 + w) * dim + d];
         }
         __syncthreads();
-        const uint32_t hit = cc_chunk(CtaGroup{}, sc, B, nw, false, full_sweep != 0);
+        const uint32_t hit = cc_chunk(CtaGroup{}, sc, B, nw, false, full_sweep != 0, par);
         for (int w = tid; w < nw; w += blockDim.x) verdicts[c0 + w] = (hit >> w) & 1u;
     }
 }

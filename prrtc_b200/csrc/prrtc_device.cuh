@@ -712,21 +712,49 @@ __device__ __forceinline__ void cc_centres(const Scene& sc, const CcBufs& B, int
     }
 }
 
-// Collision check of nw (<= CW <= 32) configurations already in B.q.  Every
-// thread of the group must call it.  edge_mode: stop all work at the first hit
+// Waypoints of an edge computed where they are needed instead of staged in
+// B.q: waypoint w of pass c is base + t*delta with t = (c + w*nchunk + 1)/G,
+// the same bits as the staged form.
+struct EdgeSrc {
+    const float* base;
+    const float* delta;
+    int G, nchunk, c;
+};
+
+__device__ __forceinline__ float cc_q(const CcBufs& B, const EdgeSrc* e, int w, int d) {
+    if (!e) return B.q[w * kDimMax + d];
+    const float t = __fdiv_rn((float)(e->c + w * e->nchunk + 1), (float)e->G);
+    return __fmaf_rn(t, e->delta[d], e->base[d]);
+}
+
+// joint_value of waypoint w
+__device__ __forceinline__ float cc_joint_value(const JointRec& jr, const CcBufs& B, const EdgeSrc* e, int w) {
+    if (jr.idx.z >= 0) return fmaf(jr.tv.w, cc_q(B, e, w, jr.idx.z), jr.tw.w);
+    if (jr.idx.y >= 0) return cc_q(B, e, w, jr.idx.y);
+    return 0.0f;
+}
+
+// Collision check of nw (<= CW <= 32) configurations: B.q, or the waypoints of
+// `edge` when given.  Every thread of the group must call it, with the same
+// `par`, which the call flips: B.hit holds two words used on alternate calls,
+// so a call clears the other word after its first barrier and no barrier is
+// needed between one call's read of its result and the next call.  Both
+// words must be zero (and `par` 0) before the first call.  edge_mode: stop all work at the first hit
 // (the whole edge is rejected).  Otherwise each configuration stops at its own
 // first hit, or never with full_sweep.  Returns the hit bit mask (bit w =
 // configuration w in collision).
 template <class G>
 __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B, int nw, bool edge_mode,
-                                    bool full_sweep) {
+                                    bool full_sweep, int& par, const EdgeSrc* edge = nullptr) {
     const BlobHeader& h = *sc.h;
     const int tid = g.rank(), T = g.size();
     const int J = h.J, S = h.S, S_pad = h.S_pad, K = h.K, Q = h.Q;
     const bool gated = h.gated != 0;
     const float inflate = __int_as_float(h.inflate_bits);
     const int KW = cdiv(K > 0 ? K : 1, 32), QW = cdiv(Q > 0 ? Q : 1, 32);
-    volatile uint32_t* vhit = B.hit;
+    uint32_t* hw = B.hit + par;
+    volatile uint32_t* vhit = hw;
+    par ^= 1;
 
     if (!h.enabled) {
         g.sync();
@@ -744,7 +772,6 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     const int n_parts_c =
         (n_obs == 0 || !gated) ? 0 : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * KC)), cdiv(n_obs, 4))));
     int* bounds_c = B.bounds + (kMaxParts + 1);
-    if (tid == 0) *vhit = 0u;
     if (n_parts > 0)
         for (int i = tid; i <= n_parts; i += T) B.bounds[i] = world_index_at(h, (int)((long long)i * ctot / n_parts));
     if (n_parts_c > 0)
@@ -771,7 +798,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
             int a = -1;
             if (act) {
                 const JointRec& jr = sc.joints[j];
-                joint_local(jr, joint_value(jr, &B.q[w * kDimMax]), X);
+                joint_local(jr, cc_joint_value(jr, B, edge, w), X);
                 const int p = jr.idx.x;
                 a = (p >= 0 && p < j) ? p : -1;
             }
@@ -801,7 +828,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         for (int it = tid; it < nw * J; it += T) {
             const int w = it / J, j = it - w * J;
             const JointRec& jr = sc.joints[j];
-            joint_local(jr, joint_value(jr, &B.q[w * kDimMax]), &B.pose[(w * J + j) * 12]);
+            joint_local(jr, cc_joint_value(jr, B, edge, w), &B.pose[(w * J + j) * 12]);
         }
         g.sync();
         // B: chain composition in topological order, one waypoint per thread
@@ -817,7 +844,8 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         for (int it = tid; it < nw * T; it += T) cc_centres(sc, B, it / T, it % T, T, J, S, S_pad, K, gated, inflate);
     }
     g.sync();
-    g.sync();
+    // every thread has read the other word's previous result by now
+    if (tid == 0) B.hit[par] = 0u;  // par was flipped: this is the word the next call uses
     unsigned long long flops = 0;
     // D: coarse pre-pass -> dirty groups and touching coarse self pairs
     if (gated) {
@@ -930,7 +958,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         // one shared-memory atomic per warp: OR the hit bits of the active lanes
         const unsigned active = __activemask();
         const unsigned bits = __reduce_or_sync(active, hit ? (1u << w) : 0u);
-        if (bits && (threadIdx.x & 31) == (__ffs(active) - 1)) atomicOr(B.hit, bits);
+        if (bits && (threadIdx.x & 31) == (__ffs(active) - 1)) atomicOr(hw, bits);
     }
     if (B.stats) {
         if (tid == 0) {
