@@ -115,9 +115,10 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const float ax = c[3 + 3 * k], ay = c[4 + 3 * k], az = c[5 + 3 * k];
-            o_wb[4 * i + k] = make_float4(ax, ay, az, -(ax * c[0] + ay * c[1] + az * c[2]));
+            const float off = -(ax * c[0] + ay * c[1] + az * c[2]);
+            o_wb[4 * i + k] = make_float4(ax * kBoxInv, ay * kBoxInv, az * kBoxInv, off * kBoxInv);
         }
-        o_wb[4 * i + 3] = make_float4(c[12], c[13], c[14], 0.0f);
+        o_wb[4 * i + 3] = make_float4(c[12] * kBoxInv, c[13] * kBoxInv, c[14] * kBoxInv, 0.0f);
     }
     float4* o_wh = reinterpret_cast<float4*>(blob + L.o_wh);
     for (int i = tid; i < Nh; i += T) {

@@ -34,6 +34,11 @@ constexpr int kObsChunk = 32;    // world primitives per work item
 constexpr int kSphChunk = PRRTC_SPH_CHUNK;  // fine spheres held in registers per work item
 constexpr int kPairChunk = 32;   // explicit self pairs per work item
 constexpr float kFar = 1.0e18f;  // centre of a sphere that can never collide
+// Box records are stored scaled by 1/kBoxScale (a power of two, so the scaling
+// is exact): the checker's relu(|l| - h) becomes a saturating add, exact for
+// any distance below kBoxScale metres (robot spheres must be smaller than that).
+constexpr float kBoxScale = 1024.0f;
+constexpr float kBoxInv = 1.0f / 1024.0f;
 
 // FP32 operations per primitive test as issued by the functions below (FFMA = 2,
 // FADD/FMUL = 1; min/max/abs and the MUFU of sin/cos/sqrt are not counted).
@@ -410,6 +415,7 @@ __device__ __forceinline__ float sphere_A(float4 c) { return fmaf(c.x, c.x, fmaf
 //   sphere     h = B + O.(c, r)        (O = -2(o, r_o), B = |o|^2 - r_o^2),  hit iff h <= -(|c|^2 - r^2)
 //   capsule    h = |e|^2 - (r + r_c)^2 (e = c - p1 - t d, t = sat(d'.c + off)), hit iff h <= 0
 //   box        h = |max(|l| - hl, 0)|^2 (l = box-frame coordinates),         hit iff h <= r^2
+//              (computed in units of kBoxScale metres: h/kBoxScale^2 against (r/kBoxScale)^2)
 //   halfspace  h = n.c - n.p                                                  hit iff h <= r
 // Three-input minimum (PTX min.f32 with three sources, sm_100): folds two
 // obstacles into a running minimum with one instruction.
@@ -438,14 +444,17 @@ __device__ __forceinline__ void h_capsule(float (&h)[NS], const float4 (&c)[NS],
     }
 }
 
+// Box rows and half extents arrive scaled by kBoxInv, so l/kBoxScale and
+// h/kBoxScale: sat(|l| - h) is relu(|l| - h)/kBoxScale (one saturating add
+// instead of a subtract and a max) and h is |q|^2/kBoxScale^2, bit for bit.
 template <int NS>
 __device__ __forceinline__ void h_box(float (&h)[NS], const float4 (&c)[NS], float4 a1, float4 a2, float4 a3,
                                       float4 hl) {
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-        const float q1 = fmaxf(fabsf(fmaf(a1.x, c[k].x, fmaf(a1.y, c[k].y, fmaf(a1.z, c[k].z, a1.w)))) - hl.x, 0.0f);
-        const float q2 = fmaxf(fabsf(fmaf(a2.x, c[k].x, fmaf(a2.y, c[k].y, fmaf(a2.z, c[k].z, a2.w)))) - hl.y, 0.0f);
-        const float q3 = fmaxf(fabsf(fmaf(a3.x, c[k].x, fmaf(a3.y, c[k].y, fmaf(a3.z, c[k].z, a3.w)))) - hl.z, 0.0f);
+        const float q1 = __saturatef(fabsf(fmaf(a1.x, c[k].x, fmaf(a1.y, c[k].y, fmaf(a1.z, c[k].z, a1.w)))) - hl.x);
+        const float q2 = __saturatef(fabsf(fmaf(a2.x, c[k].x, fmaf(a2.y, c[k].y, fmaf(a2.z, c[k].z, a2.w)))) - hl.y);
+        const float q3 = __saturatef(fabsf(fmaf(a3.x, c[k].x, fmaf(a3.y, c[k].y, fmaf(a3.z, c[k].z, a3.w)))) - hl.z);
         h[k] = fmaf(q1, q1, fmaf(q2, q2, q3 * q3));
     }
 }
@@ -603,7 +612,7 @@ __device__ __forceinline__ uint32_t obstacles_vs_spheres(const Scene& sc, int j0
     hi = min(j1, base + h.Nb) - base;
     if (lo < hi) {
 #pragma unroll
-        for (int k = 0; k < NS; ++k) thr[k] = s[k].w * s[k].w;
+        for (int k = 0; k < NS; ++k) thr[k] = (s[k].w * kBoxInv) * (s[k].w * kBoxInv);
         const float4* wb = sc.wb;
         if (sweep_type<NS, FULL, PAIRS>(m, thr, lo, hi, [&](float (&v)[NS], int o) { h_box<NS>(v, s, wb[4 * o], wb[4 * o + 1], wb[4 * o + 2], wb[4 * o + 3]); }, done))
             mask |= le_mask(m, thr);

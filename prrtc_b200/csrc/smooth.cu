@@ -125,8 +125,13 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
             gx = fmaf(k, ex, gx); gy = fmaf(k, ey, gy); gz = fmaf(k, ez, gz);
         }
         for (int o = 0; o < h.Nb; ++o) {
-            const float4 ax[3] = {sc.wb[4 * o], sc.wb[4 * o + 1], sc.wb[4 * o + 2]};
-            const float4 hl = sc.wb[4 * o + 3];
+            // records are stored scaled by 1/kBoxScale (a power of two): undo exactly
+            float4 ax[3] = {sc.wb[4 * o], sc.wb[4 * o + 1], sc.wb[4 * o + 2]};
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                ax[k] = make_float4(ax[k].x * kBoxScale, ax[k].y * kBoxScale, ax[k].z * kBoxScale, ax[k].w * kBoxScale);
+            float4 hl = sc.wb[4 * o + 3];
+            hl = make_float4(hl.x * kBoxScale, hl.y * kBoxScale, hl.z * kBoxScale, 0.0f);
             const float hh[3] = {hl.x, hl.y, hl.z};
             float l[3], qv[3], out2 = 0.0f, qmax = -INFINITY;
             int kmax = 0;
