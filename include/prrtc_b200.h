@@ -107,7 +107,8 @@ typedef struct {
     int32_t* completed;          /* [2]                        / [B,2] */
     int32_t* iter_count;         /* [1]                        / [B,1] */
     int32_t* connection_info;    /* [3]                        / [B,3] */
-    int32_t* solved_flag;        /* [1]  1 solved, 0, -1 failed / [B,1] */
+    int32_t* solved_flag;        /* [1]  1 solved, 0, -1 failed / [B,1]; -2: stopped because a
+                                    device-side wait ran out (see prrtc_tuning_t) */
     float* kernel_time_ms;       /* [1]                        / [B]  device-clock solve time */
 } prrtc_outputs_t;
 
@@ -165,6 +166,11 @@ typedef struct {
                                     idle CTAs join problems still running as extra explorers
                                     (own Halton sequences); 0 = on (default), -1 = off, so
                                     every problem keeps exactly num_new_samples explorers */
+    int32_t staging_wait_polls;  /* polls of each CTA's scene-staging wait before it gives up, after
+                                    which the planner stops with solved_flag -2 on every open
+                                    problem: 0 = default (about 4 million), > 0 = that many,
+                                    < 0 = none (the wait gives up at once: tests the failure
+                                    path without a fault) */
 } prrtc_tuning_t;
 
 size_t prrtc_b200_plan_workspace_size(const prrtc_inputs_t* in, const prrtc_attrs_t* attrs,

@@ -251,10 +251,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
 constexpr int kWaitLimit = 1 << 22;
 
 // Bulk-copy `bytes` (multiple of 16; both addresses 16-byte aligned) from global
-// memory into shared memory and wait for completion with a bounded spin.  All
-// threads call it; returns false (uniformly) if the copy did not complete.
+// memory into shared memory and wait for completion with a bounded spin of
+// `first_limit` polls.  All threads call it; returns false (uniformly) if the
+// wait ran out, after setting *err and giving the copy a second bounded wait to
+// land.
 __device__ bool stage_blob(unsigned char* dst, const unsigned char* src, int bytes, uint64_t* mbar,
-                           uint32_t& phase, int* err) {
+                           uint32_t& phase, int* err, int first_limit) {
     __syncthreads();  // previous readers of dst are done
     if (threadIdx.x == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -274,14 +276,17 @@ __device__ bool stage_blob(unsigned char* dst, const unsigned char* src, int byt
         }
     }
     bool ok = false;
-    for (int i = 0; i < kWaitLimit && !ok; ++i) ok = mbar_try_wait(mbar, phase);
-    if (!ok) {
-        if (err) atomicExch(err, 1);
-        // give the copy a second bounded chance to land before the CTA moves on
+    for (int i = 0; i < first_limit && !ok; ++i) ok = mbar_try_wait(mbar, phase);
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!all_ok) {
+        // the wait ran out: report it, then let the copy land (bounded) before
+        // the CTA stops using -- or leaves -- its shared memory
+        if (threadIdx.x == 0 && err) atomicExch(err, 1);
         for (int i = 0; i < kWaitLimit && !ok; ++i) ok = mbar_try_wait(mbar, phase);
+        __syncthreads();
     }
     phase ^= 1u;
-    return __syncthreads_and(ok ? 1 : 0) != 0;
+    return all_ok;
 }
 
 // ============================================================================ nearest neighbour
@@ -709,7 +714,7 @@ __global__ void __launch_bounds__(256) explore_kernel(PlanLaunch L) {
         if (b != cur) {
             if (staged) {
                 const int bytes = reinterpret_cast<const BlobHeader*>(gblob)->used_bytes;
-                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1])) break;
+                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1], L.wait_polls == 0 ? kWaitLimit : max(L.wait_polls, 0))) break;
                 sc = scene_view(blob_sm);
             } else {
                 sc = scene_view(gblob);
@@ -782,7 +787,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) explore_warps_kernel(PlanLa
         if (b != cur) {
             if (staged) {
                 const int bytes = reinterpret_cast<const BlobHeader*>(gblob)->used_bytes;
-                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1])) break;
+                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1], L.wait_polls == 0 ? kWaitLimit : max(L.wait_polls, 0))) break;
                 sc = scene_view(blob_sm);
             } else {
                 sc = scene_view(gblob);
@@ -833,6 +838,9 @@ __global__ void finalize_kernel(PlanLaunch L) {
     if (b >= L.B) return;
     const unsigned long long t0 = L.tstamp[2 * b], t1 = L.tstamp[2 * b + 1];
     L.ktime[b] = (t1 > t0 && t0 != 0ull) ? (float)((double)(t1 - t0) * 1e-6) : 0.0f;
+    // a device wait ran out somewhere in the launch: problems left open are
+    // reported as -2 instead of the "still running" 0
+    if (L.queue[1] != 0 && L.solved[b] == 0) L.solved[b] = -2;
 }
 
 size_t plan_workspace_bytes(int B, int N, size_t blob_stride) {

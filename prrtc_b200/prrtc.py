@@ -182,6 +182,9 @@ class _Results:
         """One read-back of the [B,16] scalar block (plus, with paths_on_host, one
         bulk copy of every path) and the per-problem PRRTCResults."""
         host = self.block.cpu().numpy()
+        if (host[:, 8] == -2).any():
+            raise _lib.PrrtcError("a device-side wait ran out (scene staging): the planner stopped and these "
+                                  "results are incomplete")
         hpaths = None
         if paths_on_host:
             lmax = int(max(0, host[:, 10].max())) if self.B else 0

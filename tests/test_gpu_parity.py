@@ -429,3 +429,25 @@ def test_async_batches_on_two_streams(cuda, orc):
             if r.solved:
                 ok, md = orc.Scene(p.context, p.dim).validate_path(r.path.numpy(), 0.01)
                 assert ok, md
+
+
+def test_staging_wait_that_runs_out_reports_minus_two(cuda):
+    """Failure path of the bounded scene-staging wait, without a fault: with no
+    polls allowed every CTA's wait gives up at once (its copy still lands
+    before the CTA leaves), the open problems come back as solved_flag -2 and
+    the Python layer raises; the same planner then runs normally."""
+    from prrtc_b200._lib import PrrtcError
+    from prrtc_b200.batch import BatchPlanner, PlanSettings
+
+    probs = [make_problem("uneven", 500 + i) for i in range(3)]
+    pl = BatchPlanner(probs, 16384, PlanSettings(num_new_samples=2), cuda)
+    pl.tun.staging_wait_polls = -1
+    pl.launch()
+    blk = pl.summary_block().cpu().numpy()
+    assert (blk[:, 8] == -2).all()
+    with pytest.raises(PrrtcError):
+        pl.results()
+    pl.tun.staging_wait_polls = 0
+    pl.launch()
+    res = pl.results()
+    assert sum(r.solved for r in res) >= len(probs) - 1
