@@ -451,3 +451,23 @@ def test_staging_wait_that_runs_out_reports_minus_two(cuda):
     pl.launch()
     res = pl.results()
     assert sum(r.solved for r in res) >= len(probs) - 1
+
+
+@pytest.mark.parametrize("batch", [1, 3])
+def test_nearest_neighbor_large_tree(cuda, orc, batch):
+    """1-3 queries over a 117 MB tree (larger than L2): a ragged tree size, NaN
+    slots and a duplicated node (ties go to the lowest index) match the oracle."""
+    from prrtc_b200 import prrtc_nearest_neighbor
+
+    rng = np.random.default_rng(31 + batch)
+    dim, N, n = 7, 1 << 22, (1 << 22) - 12345
+    tree = np.full((dim, N), np.nan, np.float32)
+    tree[:, :n] = rng.uniform(-2.8, 2.8, (dim, n)).astype(np.float32)
+    q = rng.uniform(-2.8, 2.8, (batch, dim)).astype(np.float32)
+    tree[:, n - 7] = q[0]          # an exact hit near the end ...
+    tree[:, 1000] = q[0]           # ... and the same node earlier: index 1000 wins
+    dist, idx = prrtc_nearest_neighbor(torch.from_numpy(tree).to(cuda), torch.from_numpy(q).to(cuda), n)
+    oi, od = orc.nearest_batch(tree, n, q)
+    assert idx.cpu().numpy().tolist() == oi.tolist()
+    assert idx[0].item() == 1000 and dist[0].item() == 0.0
+    assert np.array_equal(dist.cpu().numpy().view(np.uint32), np.sqrt(od.astype(np.float32)).view(np.uint32))
