@@ -76,3 +76,53 @@ def choose(problems, N: int, settings, dev, candidates=CANDIDATES, use_cache: bo
         except OSError:
             pass
     return best
+
+
+def choose_joint(buckets: dict, tuned: dict, settings, dev, samples=(1, 2, 4), reps: int = 3) -> dict:
+    """Explorers per problem for every bucket at once, timed the way the buckets
+    run: concurrently, one stream each.  ``tuned`` holds each bucket's own
+    choice (``choose``), whose threads and waypoint chunk are kept; the
+    candidates are every combination of ``samples`` across the buckets, and a
+    combination must beat the incumbent (the per-bucket choices) by 3%.
+    Returns a new {max_nodes: settings dict}."""
+    from itertools import product
+
+    from .batch import BatchPlanner, PlanSettings
+
+    Ns = list(buckets)
+    planners = {}
+    for N in Ns:
+        for E in set(samples) | {tuned[N]["num_new_samples"]}:
+            s = PlanSettings(**{**settings.__dict__, **tuned[N], "num_new_samples": E})
+            planners[(N, E)] = BatchPlanner(buckets[N], N, s, dev)
+    streams = [torch.cuda.Stream(device=dev) for _ in Ns]
+
+    def rate(combo) -> float:
+        main = torch.cuda.current_stream(dev)
+        rates = []
+        for _ in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(main)
+            for st, N, E in zip(streams, Ns, combo):
+                st.wait_event(e0)
+                with torch.cuda.stream(st):
+                    planners[(N, E)].launch()
+            for st in streams:
+                main.wait_stream(st)
+            e1.record(main)
+            e1.synchronize()
+            solved = sum(int((planners[(N, E)].summary_block()[:, 8] == 1).sum().item()) for N, E in zip(Ns, combo))
+            rates.append(solved / (e0.elapsed_time(e1) * 1e-3))
+        return sorted(rates[1:])[reps // 2]  # first run is a warm-up
+
+    base = tuple(tuned[N]["num_new_samples"] for N in Ns)
+    best, best_rate = base, rate(base)
+    for combo in product(samples, repeat=len(Ns)):
+        if combo == base:
+            continue
+        r = rate(combo)
+        if r > best_rate * 1.03:
+            best, best_rate = combo, r
+    del planners
+    torch.cuda.synchronize(dev)
+    return {N: {**tuned[N], "num_new_samples": E} for N, E in zip(Ns, best)}
