@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-launch / CC / NN side measurements")
     ap.add_argument("--eager", action="store_true", help="launch every step eagerly instead of replaying graphs")
+    ap.add_argument("--launch", choices=["merged", "buckets"], default="merged",
+                    help="one launch for every problem with per-problem tree capacities (merged), or one "
+                         "launch per capacity bucket on concurrent streams (buckets)")
     ap.add_argument("--tune", choices=["joint", "bucket"], default="bucket",
                     help="explorer counts tuned per bucket alone (default; measured 144 K vs 139-143 K plans/s) "
                          "or with the buckets running together (joint)")
@@ -282,14 +285,22 @@ def run_ours(a):
     from prrtc_b200.autotune import choose, choose_joint
 
     buckets = bucket_problems(problems)
-    tuned = {N: choose(ps, N, settings, dev) for N, ps in buckets.items()}
+    if a.launch == "merged":
+        # every problem in one launch and one work queue (tail join reaches all
+        # of them), each tree bounded by its own bucket's capacity
+        groups = {"all": problems}
+        cap_of = {"all": [p.max_nodes for p in problems]}
+    else:
+        groups = dict(buckets)
+        cap_of = {N: N for N in buckets}
+    tuned = {k: choose(ps, cap_of[k], settings, dev) for k, ps in groups.items()}
     # optional: settle the explorer counts with the buckets running together
-    if a.tune == "joint":
+    if a.tune == "joint" and a.launch == "buckets":
         tuned = choose_joint(buckets, tuned, settings, dev)
     planners = {}
-    for N, ps in buckets.items():
-        s = PlanSettings(**{**settings.__dict__, **tuned[N]})
-        planners[N] = BatchPlanner(ps, N, s, dev)
+    for k, ps in groups.items():
+        s = PlanSettings(**{**settings.__dict__, **tuned[k]})
+        planners[k] = BatchPlanner(ps, cap_of[k], s, dev)
     flush = torch.empty(int(256 * 2**20) // 4, dtype=torch.float32, device=dev)
     # buckets run concurrently, one stream each, so one bucket's tail overlaps the others
     streams = [torch.cuda.Stream(device=dev) for _ in planners]
@@ -367,15 +378,17 @@ def run_ours(a):
                    "tuned": {str(N): v for N, v in tuned.items()},
                    "collision_checker": settings.collision_checker, "edge_resolution": settings.edge_resolution,
                    "threads_per_explorer": settings.threads_per_explorer, "l2": "flushed (256 MB write) between steps",
-                   "launch": "eager" if a.eager else "one CUDA graph per bucket",
+                   "launch": ("eager" if a.eager else "CUDA graph replay") + (
+                       ", one launch for all problems with per-problem tree capacities" if a.launch == "merged"
+                       else ", one launch per capacity bucket on concurrent streams"),
                    "parallelism": f"weak scaling, {ws} rank(s), problems sharded by rank"},
         "success_rate": success,
         "p50_solve_ms": float(np.median(solve_ms)) if solve_ms.size else None,
     }
-    line["gpu_launches"] = sum(5 + 3 for _ in planners) * a.steps  # pack, init, explore, finalize, paths + 3 torch copies
+    line["gpu_launches"] = 5 * len(planners) * a.steps  # per planner: pack, init, explore, finalize, paths
 
     if rank == 0 and not a.no_extras:
-        line.update(extras(a, torch, lib, dev, problems, planners, settings, tuned, line))
+        line.update(extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of))
     if rank == 0:
         line["clocks"] = clk.summary()
         print(json.dumps(line))
@@ -387,7 +400,7 @@ def run_ours(a):
     return 0
 
 
-def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
+def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of):
     """Side measurements on rank 0: roofline of the planner kernel, e2e through the
     public API, the plain per-problem launch form, standalone CC and NN kernels,
     and the CPU baseline."""
@@ -406,7 +419,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
     ms = 0.0
     for N, pl in planners.items():
         s = PlanSettings(**{**settings.__dict__, **tuned[N]})
-        ip = BatchPlanner(pl.problems, N, s, dev, stats=True)
+        ip = BatchPlanner(pl.problems, cap_of[N], s, dev, stats=True)
         ip.launch()
         torch.cuda.synchronize()
         ip.stats.zero_()
@@ -433,43 +446,47 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
     # --- e2e through the public API with host inputs (numpy), results + paths back to host
     from prrtc_b200 import device as _device
 
-    host_in = {}
-    for N, pl in planners.items():
-        ps = pl.problems
-        G = max(p.goals.shape[0] for p in ps)
-        goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
-        for i, p in enumerate(ps):
-            goals[i, : p.goals.shape[0]] = p.goals
-        host_in[N] = (np.stack([p.start for p in ps]), goals, [p.context for p in ps],
-                      [p.goals.shape[0] for p in ps])
-
-    e2e_streams = {N: torch.cuda.Stream(device=dev) for N in planners}
+    # The public call is split into K round-robin slices of the problems, each
+    # queued on its own stream: the host prepares slice k+1 while slice k runs.
+    K_E2E = 4
+    slices = []
+    for key, pl in planners.items():
+        caps = cap_of[key]
+        for j in range(K_E2E):
+            idx = list(range(j, len(pl.problems), K_E2E))
+            if not idx:
+                continue
+            ps = [pl.problems[i] for i in idx]
+            G = max(p.goals.shape[0] for p in ps)
+            goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
+            for i, p in enumerate(ps):
+                goals[i, : p.goals.shape[0]] = p.goals
+            cap = [caps[i] for i in idx] if isinstance(caps, list) else caps
+            slices.append((key, ps, np.stack([p.start for p in ps]), goals, [p.context for p in ps],
+                           [p.goals.shape[0] for p in ps], cap))
+    e2e_streams = [torch.cuda.Stream(device=dev) for _ in slices]
 
     def e2e_step():
-        # every bucket queued on its own stream first, then the results read
-        # back: the host prepares bucket k+1 while bucket k runs
         solved, d2h = 0, 0
-        pending = {}
+        pending = []
         main = torch.cuda.current_stream()
-        for N, pl in planners.items():
-            ps = pl.problems
-            starts, goals, ctxs, gcounts = host_in[N]
-            e2e_streams[N].wait_stream(main)
-            with torch.cuda.stream(e2e_streams[N]):
-                pending[N] = prrtc_plan_batch_async(
+        for st, (key, ps, starts, goals, ctxs, gcounts, cap) in zip(e2e_streams, slices):
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                pending.append(prrtc_plan_batch_async(
                     starts, goals, max_iterations=settings.max_iterations,
-                    num_new_samples=tuned[N]["num_new_samples"], waypoint_chunk=tuned[N]["waypoint_chunk"],
-                    max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper, collision_context=ctxs,
+                    num_new_samples=tuned[key]["num_new_samples"], waypoint_chunk=tuned[key]["waypoint_chunk"],
+                    max_nodes=cap, min_vals=ps[0].lower, max_vals=ps[0].upper, collision_context=ctxs,
                     collision_checker=settings.collision_checker, goal_counts=gcounts,
                     edge_resolution=settings.edge_resolution,
-                    threads_per_explorer=tuned[N]["threads_per_explorer"], return_trees=False, paths_on_host=True)
-        for N, pl in planners.items():
-            ps = pl.problems
-            res = pending[N].results()
+                    threads_per_explorer=tuned[key]["threads_per_explorer"], return_trees=False,
+                    paths_on_host=True))
+        for pend, (key, ps, *_rest) in zip(pending, slices):
+            res = pend.results()
             solved += sum(r.solved for r in res)
             lmax = max((r.path.shape[0] for r in res if r.solved), default=0)
             d2h += len(ps) * 16 * 4 + len(ps) * lmax * ps[0].dim * 4
-        for st in e2e_streams.values():
+        for st in e2e_streams:
             main.wait_stream(st)
         return solved, d2h
 
@@ -488,15 +505,16 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line):
     out["e2e"] = {"value": solved / dt, "unit": "plans/s", "h2d_bytes_per_step": _device.H2D_BYTES[0] // k_e2e,
                   "d2h_bytes_per_step": d2h // k_e2e, "steps": k_e2e,
                   "api": "prrtc_b200.prrtc_plan_batch_async + .results() (per-problem collision_context dicts, "
-                         "host numpy inputs, one call per capacity bucket on its own stream, paths copied to "
-                         "the host)"}
+                         "host numpy inputs, four calls over round-robin slices of the problems, each on its "
+                         "own stream, paths copied to the host)"}
 
     # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     solved_plain = 0
-    for N, pl in planners.items():
-        ps = pl.problems
+    from prrtc_b200.batch import bucket_problems
+
+    for N, ps in bucket_problems(problems).items():
         G = max(p.goals.shape[0] for p in ps)
         goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
         for i, p in enumerate(ps):

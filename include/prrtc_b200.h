@@ -203,6 +203,10 @@ typedef struct {
     const float* world_halfspaces;   int32_t max_world_halfspaces;  const int32_t* world_halfspaces_count;
     const int32_t* self_pairs;       int32_t max_self_pairs;        const int32_t* self_pairs_count;
     const int32_t* problem_order;    /* [B] or NULL */
+    const int32_t* problem_capacity; /* [B] or NULL: each problem's tree capacity (clamped to
+                                        [1, max_nodes]); its tree overflows (solved_flag -1)
+                                        there, while the outputs keep the max_nodes row stride.
+                                        Lets problems of different capacity share one launch. */
 } prrtc_batch_inputs_t;
 
 size_t prrtc_b200_plan_batch_workspace_size(const prrtc_batch_inputs_t* in, const prrtc_attrs_t* attrs,

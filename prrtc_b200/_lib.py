@@ -87,7 +87,7 @@ class BatchInputs(C.Structure):
         ("world_boxes", P), ("max_world_boxes", I32), ("world_boxes_count", P),
         ("world_halfspaces", P), ("max_world_halfspaces", I32), ("world_halfspaces_count", P),
         ("self_pairs", P), ("max_self_pairs", I32), ("self_pairs_count", P),
-        ("problem_order", P),
+        ("problem_order", P), ("problem_capacity", P),
     ]
 
 

@@ -27,6 +27,9 @@ CACHE = Path(os.environ.get("PRRTC_B200_CACHE", Path.home() / ".cache" / "prrtc_
 def _key(dev, N, problems, settings) -> str:
     p = problems[0]
     name = torch.cuda.get_device_name(dev)
+    if not isinstance(N, int):  # per-problem capacities
+        caps = [int(c) for c in N]
+        N = f"caps{max(caps)}x{len(caps)}h{hash(tuple(caps)) & 0xffffff:06x}"
     return (f"{name}|N{N}|B{len(problems)}|dim{p.dim}|S{p.context['sphere_radius'].shape[0]}|"
             f"{settings.collision_checker}|res{settings.edge_resolution}|T{settings.threads_per_explorer}")
 
@@ -38,8 +41,9 @@ def _load() -> dict:
         return {}
 
 
-def choose(problems, N: int, settings, dev, candidates=CANDIDATES, use_cache: bool = True) -> dict:
-    """Best {num_new_samples, threads_per_explorer, waypoint_chunk} for this bucket."""
+def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = True) -> dict:
+    """Best {num_new_samples, threads_per_explorer, waypoint_chunk} for this bucket
+    (N: one tree capacity, or a per-problem list of them)."""
     from .batch import BatchPlanner, PlanSettings
 
     key = "v5|" + _key(dev, N, problems, settings)

@@ -53,6 +53,11 @@ class BatchPlanner:
         self.problems = list(problems)
         B = self.B = len(self.problems)
         dim = self.dim = self.problems[0].dim
+        # an int, or one capacity per problem (one launch; row stride = the largest)
+        caps = None
+        if isinstance(max_nodes, (list, tuple, np.ndarray)):
+            caps = np.asarray(max_nodes, dtype=np.int32).reshape(B)
+            max_nodes = int(caps.max())
         self.N = int(max_nodes)
         G = max(p.goals.shape[0] for p in self.problems)
         # ---- host staging (pinned) ----
@@ -72,6 +77,8 @@ class BatchPlanner:
         for k in packed:
             self.host[k] = packed[k]
             self.host[k + "_count"] = counts[k]
+        if caps is not None:
+            self.host["caps"] = caps
         self.pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in self.host.items()}
         self.d = {k: torch.empty_like(v, device=self.dev) for k, v in self.pinned.items()}
         self.upload()
@@ -91,6 +98,8 @@ class BatchPlanner:
             setattr(bi, "max_" + key, n)
             setattr(bi, key + "_count", d[key + "_count"].data_ptr())
         bi.problem_order = d["order"].data_ptr()
+        if caps is not None:
+            bi.problem_capacity = d["caps"].data_ptr()
         self.bi = bi
         s = settings
         self.attrs = _attrs(s.max_iterations, s.step_size, s.num_new_samples, s.balance_mode, s.tree_ratio,

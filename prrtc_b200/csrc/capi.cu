@@ -257,6 +257,7 @@ int prrtc_b200_plan_batch(const prrtc_batch_inputs_t* in, const prrtc_outputs_t*
     L.pairs = in->self_pairs;
     L.pairs_stride = in->self_pairs_count ? (size_t)std::max(0, in->max_self_pairs) : 0;
     L.order = in->problem_order;
+    L.caps = in->problem_capacity;
     L.persistent = 1;
     cudaError_t e = launch_pack(s, in->batch, L.blobs, stride, st);
     if (e != cudaSuccess) return cuda_fail(e);

@@ -57,6 +57,7 @@ struct PlanLaunch {
     const float* lo; const float* hi;
     const int32_t* pairs; size_t pairs_stride;   // explicit self pairs (elements of int2 per problem)
     const int32_t* order;
+    const int32_t* caps;                         // per-problem tree capacity (<= N) or null
     // workspace
     unsigned char* blobs; size_t blob_stride; int blob_cap;
     float* radii;                      // [B][2][N]

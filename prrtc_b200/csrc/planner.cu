@@ -372,6 +372,7 @@ __device__ void group_nearest(const G& grp, const float* __restrict__ tree, int 
 // ============================================================================ explorer
 
 struct Prob {
+    int cap;  // this problem's tree capacity (<= the row stride N)
     float* tree[2];
     int* par[2];
     float* radii[2];
@@ -385,6 +386,7 @@ struct Prob {
 
 __device__ __forceinline__ Prob prob_ptrs(const PlanLaunch& L, int b) {
     Prob p;
+    p.cap = L.caps ? max(1, min(L.caps[b], L.N)) : L.N;
     const size_t tn = (size_t)L.dim * L.N;
     p.tree[0] = L.tree_a + (size_t)b * tn;
     p.tree[1] = L.tree_b + (size_t)b * tn;
@@ -519,7 +521,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
                 if (lane == 0) {
                     const int t = choose_tree(L.balance_mode, local_iter, e % L.E, L.E, sa, sb, L.tree_ratio, X.vamp);
                     X.t = t;
-                    X.n_t = min(t == 0 ? sa : sb, N);
+                    X.n_t = min(t == 0 ? sa : sb, P.cap);
                 }
             }
             if (lane == 0) X.stop = stop;
@@ -565,7 +567,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         // insert (prrtc_planner.cu:925-947)
         if (tid == 0) {
             const int idx = atomicAdd(&P.sizes[t], 1);
-            if (idx >= N) {
+            if (idx >= P.cap) {
                 if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
                 X.new_idx = -1;
             } else {
@@ -579,7 +581,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         if (tid < dim) __stcg(&P.tree[t][(size_t)tid * N + X.new_idx], X.cand[tid]);
         if (tid == 0) {
             atomicAdd(&P.completed[t], 1);
-            X.n_o = min(ld_volatile(&P.sizes[o]), N);
+            X.n_o = min(ld_volatile(&P.sizes[o]), P.cap);
         }
         grp.sync();
         // connect (prrtc_planner.cu:949-1043)
@@ -622,7 +624,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
                 int eidx = 0;
                 if (lane == 0) eidx = atomicAdd(&P.sizes[t], 1);
                 eidx = __shfl_sync(0xffffffffu, eidx, 0);
-                if (eidx >= N) {
+                if (eidx >= P.cap) {
                     if (lane == 0) {
                         if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
                         X.ext_idx = -1;
@@ -811,7 +813,7 @@ __global__ void init_kernel(PlanLaunch L, int stamp_start) {
     const Prob P = prob_ptrs(L, b);
     int G = L.num_goals;
     if (L.goal_counts) G = max(1, min(L.goal_counts[b], L.num_goals));
-    G = min(G, L.N);
+    G = min(G, P.cap);
     const float* st = L.starts + (size_t)b * L.dim;
     const float* gl = L.goals + (size_t)b * L.num_goals * L.dim;
     for (int d = tid; d < L.dim; d += blockDim.x) P.tree[0][(size_t)d * L.N] = st[d];

@@ -141,6 +141,7 @@ class _Results:
 
     def __init__(self, B: int, dim: int, N: int, device: torch.device, lead: tuple):
         self.B, self.dim, self.N = B, dim, N
+        self.caps = None  # per-problem tree capacities, when they differ from N
         self.ta = torch.empty(lead + (dim, N), dtype=torch.float32, device=device)
         self.tb = torch.empty(lead + (dim, N), dtype=torch.float32, device=device)
         self.pa = torch.empty(lead + (N,), dtype=torch.int32, device=device)
@@ -212,7 +213,8 @@ class _Results:
                         path = path.cpu()
             tac = tbc = tap = tbp = None
             if trees:  # per-problem views only when asked for (each is a tensor op)
-                na, nb = min(size_a, self.N), min(size_b, self.N)
+                cap = self.N if self.caps is None else min(int(self.caps[i]), self.N)
+                na, nb = min(size_a, cap), min(size_b, cap)
                 batched = self.ta.dim() == 3
                 tac = (self.ta[i] if batched else self.ta)[:, :na]
                 tbc = (self.tb[i] if batched else self.tb)[:, :nb]
@@ -457,7 +459,17 @@ def prrtc_plan_batch_async(
     per-problem dicts (robot tables from the first non-None entry; worlds and
     self pairs packed into padded tensors with counts).  ``paths_on_host``
     returns every path as a CPU tensor, copied with one bulk device->host copy.
+    ``max_nodes`` may also be a per-problem sequence of tree capacities: the
+    problems then share one launch (row stride = the largest capacity) and
+    each tree overflows at its own capacity.
     """
+    caps = None
+    if isinstance(max_nodes, (list, tuple, np.ndarray, torch.Tensor)):
+        caps = np.asarray(max_nodes.cpu() if isinstance(max_nodes, torch.Tensor) else max_nodes,
+                          dtype=np.int64).reshape(-1)
+        if caps.size == 0 or (caps < 1).any():
+            raise ValueError("per-problem max_nodes must be >= 1")
+        max_nodes = int(caps.max())
     lib = _lib.load()
     collision_mode = _resolve_collision_mode(collision_checker)
     step_size, granularity = _validate(step_size, granularity)
@@ -552,6 +564,12 @@ def prrtc_plan_batch_async(
         keep.append(ot)
         bi.problem_order = ot.data_ptr()
 
+    if caps is not None:
+        if caps.size != B:
+            raise ValueError(f"per-problem max_nodes must have batch_size ({B}) entries, got {caps.size}")
+        ct = torch.from_numpy(caps.astype(np.int32)).to(dev)
+        keep.append(ct)
+        bi.problem_capacity = ct.data_ptr()
     attrs = _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
                    dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin)
     tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk, resident_ctas, tail_explorers)
@@ -568,6 +586,7 @@ def prrtc_plan_batch_async(
         tun.point_cloud = cloud.address()
         keep.append(cloud)
     res = _Results(B, dim, int(max_nodes), dev, (B,))
+    res.caps = caps
     sp = stream_handle()
     if launch == "persistent":
         ws = workspace(lib.prrtc_b200_plan_batch_workspace_size(C.byref(bi), C.byref(attrs), C.byref(tun)), dev)
@@ -575,6 +594,8 @@ def prrtc_plan_batch_async(
         _lib.check(lib.prrtc_b200_plan_batch(C.byref(bi), C.byref(outs), C.byref(attrs), C.byref(tun),
                                              ws.data_ptr(), ws.numel(), sp), "prrtc_b200_plan_batch")
     elif launch == "per_problem":
+        if caps is not None:
+            raise ValueError("per-problem max_nodes needs launch='persistent'")
         _plan_per_problem(lib, bi, res, attrs, tun, contexts, robot_ctx, starts, goals, goal_counts, lo, hi, dev)
     else:
         raise ValueError(f"launch must be 'persistent' or 'per_problem', got {launch!r}")

@@ -56,7 +56,8 @@ def cuda():
 
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    from prrtc_b200 import _lib
+    from prrtc_b200 import _lib, build
 
+    build.build()  # no-op when the library is newer than every source; rebuilds a stale one
     _lib.load()
     return torch.device("cuda", 0)

@@ -471,3 +471,29 @@ def test_nearest_neighbor_large_tree(cuda, orc, batch):
     assert idx.cpu().numpy().tolist() == oi.tolist()
     assert idx[0].item() == 1000 and dist[0].item() == 0.0
     assert np.array_equal(dist.cpu().numpy().view(np.uint32), np.sqrt(od.astype(np.float32)).view(np.uint32))
+
+
+def test_batch_per_problem_capacity(cuda, orc):
+    """Problems of different tree capacity in one launch: each tree stays within
+    its own capacity; a capacity too small to solve overflows (solved_flag -1)
+    without affecting the others."""
+    from prrtc_b200 import prrtc_plan_batch
+
+    probs = [make_problem("uneven", 600 + i) for i in range(6)]
+    caps = [4096, 16384, 65536, 4096, 16384, 2]  # 2: any extend + connect overflows
+    G = max(p.goals.shape[0] for p in probs)
+    dim = probs[0].dim
+    goals = np.zeros((len(probs), G, dim), np.float32)
+    for i, p in enumerate(probs):
+        goals[i, : p.goals.shape[0]] = p.goals
+    res = prrtc_plan_batch(np.stack([p.start for p in probs]), goals, max_iterations=5000, num_new_samples=4,
+                           max_nodes=caps, min_vals=probs[0].lower, max_vals=probs[0].upper,
+                           collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
+                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01)
+    for p, r, cap in zip(probs, res, caps):
+        assert r.tree_a_configs.shape[1] <= cap and r.tree_b_configs.shape[1] <= cap
+        if r.solved:
+            ok, md = orc.Scene(p.context, dim).validate_path(r.path.cpu().numpy(), 0.01)
+            assert ok, md
+    assert sum(r.solved for r in res[:5]) >= 4
+    assert not res[5].solved and max(res[5].tree_a_size, res[5].tree_b_size) >= 2
