@@ -446,67 +446,65 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     # --- e2e through the public API with host inputs (numpy), results + paths back to host
     from prrtc_b200 import device as _device
 
-    # The public call is split into K round-robin slices of the problems, each
-    # queued on its own stream: the host prepares slice k+1 while slice k runs.
-    K_E2E = 4
-    slices = []
+    # One public call per step for all problems, double-buffered over two
+    # streams: the host packs and copies step k+1 while the device plans step k,
+    # then reads back step k's results.  Every step's inputs still go host ->
+    # device and its results device -> host inside the timed region.
+    calls = []
     for key, pl in planners.items():
-        caps = cap_of[key]
-        for j in range(K_E2E):
-            idx = list(range(j, len(pl.problems), K_E2E))
-            if not idx:
-                continue
-            ps = [pl.problems[i] for i in idx]
-            G = max(p.goals.shape[0] for p in ps)
-            goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
-            for i, p in enumerate(ps):
-                goals[i, : p.goals.shape[0]] = p.goals
-            cap = [caps[i] for i in idx] if isinstance(caps, list) else caps
-            slices.append((key, ps, np.stack([p.start for p in ps]), goals, [p.context for p in ps],
-                           [p.goals.shape[0] for p in ps], cap))
-    e2e_streams = [torch.cuda.Stream(device=dev) for _ in slices]
+        ps = pl.problems
+        G = max(p.goals.shape[0] for p in ps)
+        goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
+        for i, p in enumerate(ps):
+            goals[i, : p.goals.shape[0]] = p.goals
+        calls.append((key, ps, np.stack([p.start for p in ps]), goals, [p.context for p in ps],
+                      [p.goals.shape[0] for p in ps], cap_of[key]))
+    e2e_streams = [torch.cuda.Stream(device=dev) for _ in range(2)]
 
-    def e2e_step():
-        solved, d2h = 0, 0
+    def enqueue(k):
         pending = []
-        main = torch.cuda.current_stream()
-        for st, (key, ps, starts, goals, ctxs, gcounts, cap) in zip(e2e_streams, slices):
-            st.wait_stream(main)
-            with torch.cuda.stream(st):
-                pending.append(prrtc_plan_batch_async(
+        with torch.cuda.stream(e2e_streams[k % 2]):
+            for key, ps, starts, goals, ctxs, gcounts, cap in calls:
+                pending.append((ps, prrtc_plan_batch_async(
                     starts, goals, max_iterations=settings.max_iterations,
                     num_new_samples=tuned[key]["num_new_samples"], waypoint_chunk=tuned[key]["waypoint_chunk"],
                     max_nodes=cap, min_vals=ps[0].lower, max_vals=ps[0].upper, collision_context=ctxs,
                     collision_checker=settings.collision_checker, goal_counts=gcounts,
                     edge_resolution=settings.edge_resolution,
                     threads_per_explorer=tuned[key]["threads_per_explorer"], return_trees=False,
-                    paths_on_host=True))
-        for pend, (key, ps, *_rest) in zip(pending, slices):
+                    paths_on_host=True)))
+        return pending
+
+    def collect(pending):
+        solved, d2h = 0, 0
+        for ps, pend in pending:
             res = pend.results()
             solved += sum(r.solved for r in res)
             lmax = max((r.path.shape[0] for r in res if r.solved), default=0)
             d2h += len(ps) * 16 * 4 + len(ps) * lmax * ps[0].dim * 4
-        for st in e2e_streams:
-            main.wait_stream(st)
         return solved, d2h
 
-    e2e_step()  # warm: first-call allocations
+    collect(enqueue(0))  # warm: first-call allocations
+    collect(enqueue(1))
     torch.cuda.synchronize()
     _device.H2D_BYTES[0] = 0
-    k_e2e = 5
+    k_e2e = 10
     solved = d2h = 0
     t0 = time.perf_counter()
-    for _ in range(k_e2e):
-        s_, d_ = e2e_step()
+    pend = enqueue(0)
+    for k in range(k_e2e):
+        nxt = enqueue(k + 1) if k + 1 < k_e2e else None
+        s_, d_ = collect(pend)
         solved += s_
         d2h += d_
+        pend = nxt
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     out["e2e"] = {"value": solved / dt, "unit": "plans/s", "h2d_bytes_per_step": _device.H2D_BYTES[0] // k_e2e,
                   "d2h_bytes_per_step": d2h // k_e2e, "steps": k_e2e,
                   "api": "prrtc_b200.prrtc_plan_batch_async + .results() (per-problem collision_context dicts, "
-                         "host numpy inputs, four calls over round-robin slices of the problems, each on its "
-                         "own stream, paths copied to the host)"}
+                         "host numpy inputs, one call per step for all problems, double-buffered on two "
+                         "streams: step k+1 is packed and copied while step k plans; paths copied to the host)"}
 
     # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
     torch.cuda.synchronize()

@@ -93,6 +93,38 @@ def upload(arrays, device: torch.device) -> list[torch.Tensor]:
 
 
 _TORCH_DTYPE = {"f4": torch.float32, "i4": torch.int32, "u1": torch.uint8, "i8": torch.int64, "f8": torch.float64}
+_NUMPY_DTYPE = {torch.float32: np.float32, torch.int32: np.int32, torch.uint8: np.uint8, torch.int64: np.int64,
+                torch.float64: np.float64}
+
+
+class Stager:
+    """Inputs of one call gathered for a single pinned host->device copy.
+
+    ``add`` queues a host array (numpy, list, CPU tensor) and returns a key;
+    a tensor already on the device passes through without a copy.  After
+    ``commit`` (one ``upload``), ``get(key)`` is the device tensor."""
+
+    def __init__(self, device: torch.device):
+        self.device = device
+        self._host: list[np.ndarray] = []
+        self._dev: list[torch.Tensor] | None = None
+
+    def add(self, x, dtype: torch.dtype, shape=None):
+        if isinstance(x, torch.Tensor) and x.device == self.device:
+            t = x.to(dtype=dtype)
+            return ("t", (t.reshape(shape) if shape is not None else t).contiguous())
+        a = np.asarray(x.cpu() if isinstance(x, torch.Tensor) else x, dtype=_NUMPY_DTYPE[dtype])
+        if shape is not None:
+            a = a.reshape(shape)
+        self._host.append(np.ascontiguousarray(a))
+        return ("h", len(self._host) - 1)
+
+    def commit(self) -> None:
+        self._dev = upload(self._host, self.device) if self._host else []
+
+    def get(self, key) -> torch.Tensor:
+        kind, v = key
+        return v if kind == "t" else self._dev[v]
 
 
 def ptr(t: torch.Tensor | None) -> int | None:
@@ -109,17 +141,30 @@ def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
 class DeviceContext:
     """collision_context tensors on one CUDA device."""
 
-    def __init__(self, ctx: dict | None, device: torch.device, world_keys: bool = True):
+    def __init__(self, ctx: dict | None, device: torch.device, world_keys: bool = True, stager: Stager | None = None):
+        """With a ``stager``, host tables are queued on it and the tensors exist
+        after ``finish()`` (called once the stager has committed)."""
         self.device = device
         self.t: dict[str, torch.Tensor] = {}
+        self._keys: dict = {}
         spec = dict(ROBOT_SPEC)
         if world_keys:
             spec.update(WORLD_SPEC)
         for k, (dt, cols) in spec.items():
             if ctx is not None and k in ctx and ctx[k] is not None:
-                self.t[k] = as_tensor(ctx[k], dt, device, cols)
+                if stager is not None:
+                    self._keys[k] = stager.add(ctx[k], dt, (-1, cols) if cols else (-1,))
+                else:
+                    self.t[k] = as_tensor(ctx[k], dt, device, cols)
             else:
                 self.t[k] = torch.zeros((0, cols) if cols else (0,), dtype=dt, device=device)
+        self._stager = stager
+
+    def finish(self) -> "DeviceContext":
+        for k, key in self._keys.items():
+            self.t[k] = self._stager.get(key)
+        self._keys, self._stager = {}, None
+        return self
 
     def n(self, key: str) -> int:
         return int(self.t[key].shape[0])

@@ -34,7 +34,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import REQUIRED_KEYS, DeviceContext, as_tensor, cuda_device, ptr, stream_handle, upload, workspace
+from .device import REQUIRED_KEYS, DeviceContext, Stager, as_tensor, cuda_device, ptr, stream_handle, workspace
 
 _COLLISION_MODES = {"binary": 0, "differentiable": 1, "binary_coarse": 2, "binary_coarse_coop": 3}
 PATH_MAX_LEN = 16384
@@ -405,6 +405,16 @@ def _shared_table(contexts: Sequence[Optional[dict]], key: str):
 _LPT_WEIGHTS = (("world_spheres", 1.0), ("world_capsules", 2.0), ("world_boxes", 3.0), ("world_halfspaces", 1.0))
 
 
+def _lpt_from_counts(counts: dict, B: int) -> np.ndarray:
+    """lpt_order from the per-problem row counts of the packed tables (a table
+    shared by every problem adds the same cost to each and is left out)."""
+    cost = np.zeros(B, dtype=np.float64)
+    for k, w in _LPT_WEIGHTS:
+        if k in counts:
+            cost += w * counts[k]
+    return np.argsort(-cost, kind="stable").astype(np.int32)
+
+
 def lpt_order(contexts: Sequence[Optional[dict]], goal_counts=None) -> np.ndarray:
     """Longest-processing-time order: problems with the most collision work first."""
     cost = np.zeros(len(contexts), dtype=np.float64)
@@ -476,19 +486,32 @@ def prrtc_plan_batch_async(
     if collision_context is None:
         _check_context(None, allow_unsafe_no_collision)
     dev = cuda_device(device)
-    starts = as_tensor(start_configs, torch.float32, dev)
-    if starts.dim() == 1:
-        starts = starts.reshape(1, -1)
-    B, dim = int(starts.shape[0]), int(starts.shape[1])
-    goals = as_tensor(goal_configs, torch.float32, dev)
-    if goals.dim() == 2:
-        goals = goals[:, None, :]
-    if goals.dim() != 3 or goals.shape[0] != B:
-        raise ValueError(f"goal_configs must have shape (batch, num_goals, dim), got {tuple(goals.shape)} "
+    # every host input of the call (configs, limits, counts, order, capacities,
+    # robot tables, packed worlds) goes to the device in one pinned copy
+    stage = Stager(dev)
+    starts_np = starts_dev = None
+    if isinstance(start_configs, torch.Tensor) and start_configs.device == dev:
+        starts_dev = start_configs.to(torch.float32)
+        shape = tuple(starts_dev.shape)
+    else:
+        starts_np = np.asarray(start_configs.cpu() if isinstance(start_configs, torch.Tensor) else start_configs,
+                               dtype=np.float32)
+        shape = starts_np.shape
+    if len(shape) == 1:
+        shape = (1,) + shape
+    B, dim = int(shape[0]), int(shape[1])
+    k_starts = stage.add(starts_dev if starts_dev is not None else starts_np, torch.float32, (B, dim))
+    gshape = tuple(goal_configs.shape) if isinstance(goal_configs, torch.Tensor) else np.shape(goal_configs)
+    if len(gshape) == 2:
+        gshape = (gshape[0], 1, gshape[1])
+    if len(gshape) != 3 or gshape[0] != B:
+        raise ValueError(f"goal_configs must have shape (batch, num_goals, dim), got {tuple(gshape)} "
                          f"with batch_size={B}")
-    goals = goals.contiguous()
-    G = int(goals.shape[1])
-    lo, hi = _limits(min_vals, max_vals, dim, dev)
+    G = int(gshape[1])
+    k_goals = stage.add(goal_configs, torch.float32, gshape)
+    k_lo = stage.add(np.full(dim, -np.pi, np.float32) if min_vals is None else min_vals, torch.float32, (dim,))
+    k_hi = stage.add(np.full(dim, np.pi, np.float32) if max_vals is None else max_vals, torch.float32, (dim,))
+    k_gc = stage.add(goal_counts, torch.int32, (B,)) if goal_counts is not None else None
 
     per_problem = isinstance(collision_context, (list, tuple))
     if per_problem:
@@ -510,42 +533,51 @@ def prrtc_plan_batch_async(
         contexts = [collision_context] * B
         first = collision_context
 
-    robot_ctx = DeviceContext(first, dev, world_keys=not per_problem)
-    bi = _lib.BatchInputs()
-    bi.batch = B
-    bi.start_configs, bi.goal_configs, bi.num_goals = starts.data_ptr(), goals.data_ptr(), G
-    keep = []
-    if goal_counts is not None:
-        gc = as_tensor(goal_counts, torch.int32, dev).reshape(B)
-        keep.append(gc)
-        bi.goal_counts = gc.data_ptr()
-    bi.min_vals, bi.max_vals = lo.data_ptr(), hi.data_ptr()
-    bi.robot = robot_ctx.robot()
+    robot_ctx = DeviceContext(first, dev, world_keys=not per_problem, stager=stage)
+    keys = ("world_spheres", "world_capsules", "world_boxes", "world_halfspaces", "self_pairs")
+    world_keys, counts = {}, None
     if per_problem and first is not None:
-        keys = ("world_spheres", "world_capsules", "world_boxes", "world_halfspaces", "self_pairs")
         # a table every problem shares (typically the robot's self pairs) goes
         # once, unbatched, with no count pointer
         shared = {k: _shared_table(contexts, k) for k in keys}
         packed, counts = _pack_worlds(contexts, B, skip={k for k in keys if shared[k] is not None})
-        host = []
         for key in keys:
             if shared[key] is not None:
-                host.append(shared[key])
+                world_keys[key] = (stage.add(shared[key], torch.int32 if key == "self_pairs" else torch.float32),
+                                   None, int(shared[key].shape[0]))
             else:
-                host += [packed[key], counts[key]]
-        dev_t = iter(upload(host, dev))
-        for key in keys:
-            t = next(dev_t)
-            keep.append(t)
-            setattr(bi, key, ptr(t))
-            if shared[key] is not None:
-                setattr(bi, "max_" + key, int(shared[key].shape[0]))
-                setattr(bi, key + "_count", None)
-            else:
-                c = next(dev_t)
-                keep.append(c)
-                setattr(bi, "max_" + key, int(packed[key].shape[1]))
-                setattr(bi, key + "_count", ptr(c))
+                world_keys[key] = (stage.add(packed[key], torch.int32 if key == "self_pairs" else torch.float32),
+                                   stage.add(counts[key], torch.int32), int(packed[key].shape[1]))
+    order = None
+    if isinstance(problem_order, str):
+        if problem_order == "auto" and per_problem:
+            # longest-processing-time order from the packed counts (same order as lpt_order)
+            order = _lpt_from_counts(counts, B) if counts is not None else lpt_order(contexts)
+    elif problem_order is not None:
+        order = np.asarray(problem_order, dtype=np.int32).reshape(B)
+    k_order = stage.add(order, torch.int32) if order is not None else None
+    k_caps = None
+    if caps is not None:
+        if caps.size != B:
+            raise ValueError(f"per-problem max_nodes must have batch_size ({B}) entries, got {caps.size}")
+        k_caps = stage.add(caps, torch.int32)
+    stage.commit()
+    robot_ctx.finish()
+
+    starts, goals, lo, hi = stage.get(k_starts), stage.get(k_goals), stage.get(k_lo), stage.get(k_hi)
+    bi = _lib.BatchInputs()
+    bi.batch = B
+    bi.start_configs, bi.goal_configs, bi.num_goals = starts.data_ptr(), goals.data_ptr(), G
+    keep = [stage]
+    if k_gc is not None:
+        bi.goal_counts = stage.get(k_gc).data_ptr()
+    bi.min_vals, bi.max_vals = lo.data_ptr(), hi.data_ptr()
+    bi.robot = robot_ctx.robot()
+    if world_keys:
+        for key, (k_tab, k_cnt, width) in world_keys.items():
+            setattr(bi, key, ptr(stage.get(k_tab)))
+            setattr(bi, "max_" + key, width)
+            setattr(bi, key + "_count", ptr(stage.get(k_cnt)) if k_cnt is not None else None)
     elif first is not None:
         w = robot_ctx.world()
         bi.world_spheres, bi.max_world_spheres = w.world_spheres, w.n_world_spheres
@@ -553,23 +585,10 @@ def prrtc_plan_batch_async(
         bi.world_boxes, bi.max_world_boxes = w.world_boxes, w.n_world_boxes
         bi.world_halfspaces, bi.max_world_halfspaces = w.world_halfspaces, w.n_world_halfspaces
         bi.self_pairs, bi.max_self_pairs = w.self_pairs, w.n_self_pairs
-    order = None
-    if isinstance(problem_order, str):
-        if problem_order == "auto" and per_problem:
-            order = lpt_order(contexts)
-    elif problem_order is not None:
-        order = np.asarray(problem_order, dtype=np.int32).reshape(B)
-    if order is not None:
-        ot = torch.from_numpy(np.ascontiguousarray(order)).to(dev)
-        keep.append(ot)
-        bi.problem_order = ot.data_ptr()
-
-    if caps is not None:
-        if caps.size != B:
-            raise ValueError(f"per-problem max_nodes must have batch_size ({B}) entries, got {caps.size}")
-        ct = torch.from_numpy(caps.astype(np.int32)).to(dev)
-        keep.append(ct)
-        bi.problem_capacity = ct.data_ptr()
+    if k_order is not None:
+        bi.problem_order = stage.get(k_order).data_ptr()
+    if k_caps is not None:
+        bi.problem_capacity = stage.get(k_caps).data_ptr()
     attrs = _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
                    dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin)
     tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk, resident_ctas, tail_explorers)
@@ -601,7 +620,7 @@ def prrtc_plan_batch_async(
         raise ValueError(f"launch must be 'persistent' or 'per_problem', got {launch!r}")
     res.extract(sp)
     # everything the queued kernels read stays referenced until results()
-    keep += [starts, goals, lo, hi, robot_ctx] + ([ws] if launch == "persistent" else [])
+    keep += [robot_ctx] + ([ws] if launch == "persistent" else [])
     return PendingBatch(res, keep, torch.cuda.current_stream(dev), return_trees, paths_on_host)
 
 
