@@ -154,6 +154,22 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     return lib
 
 
+_hostpack = None
+
+
+def hostpack():
+    """The native host packer module (csrc/hostpack.cc), built on first use."""
+    global _hostpack
+    if _hostpack is None:
+        from . import build as _build
+
+        _build.build_hostpack()
+        from . import _hostpack as hp
+
+        _hostpack = hp
+    return _hostpack
+
+
 class PrrtcError(RuntimeError):
     pass
 

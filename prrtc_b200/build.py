@@ -1,8 +1,11 @@
-"""Build libprrtc_b200.so (sm_100a) in-tree with nvcc.
+"""Build libprrtc_b200.so (sm_100a) in-tree with nvcc, and the host packer
+module ``_hostpack`` with g++.
 
 Each ``csrc/*.cu`` is compiled to an object in ``prrtc_b200/_build/`` (in
-parallel), then linked into ``prrtc_b200/libprrtc_b200.so``.  Rebuilds only
-when a source or header is newer than the library.
+parallel), then linked into ``prrtc_b200/libprrtc_b200.so``;
+``csrc/hostpack.cc`` (CPython C API, no CUDA) becomes
+``prrtc_b200/_hostpack<EXT_SUFFIX>``.  Each rebuilds only when a source or
+header is newer than its output.
 """
 from __future__ import annotations
 
@@ -11,6 +14,7 @@ import os
 import shutil
 import subprocess
 import sys
+import sysconfig
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -18,6 +22,8 @@ CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libprrtc_b200.so"
 INCLUDE = HERE.parent / "include"
+HOSTPACK_SRC = CSRC / "hostpack.cc"
+HOSTPACK = HERE / ("_hostpack" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -47,7 +53,24 @@ def up_to_date() -> bool:
     return all(p.stat().st_mtime <= t for p in _deps())
 
 
+def build_hostpack(force: bool = False) -> Path:
+    """g++ -O2 -shared of the CPython host packer."""
+    if not force and HOSTPACK.exists() and all(
+            p.stat().st_mtime <= HOSTPACK.stat().st_mtime for p in (HOSTPACK_SRC, Path(__file__))):
+        return HOSTPACK
+    cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+    tmp = HOSTPACK.with_name(HOSTPACK.name + ".tmp")
+    cmd = [cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fno-strict-aliasing", "-Wall",
+           "-I", sysconfig.get_paths()["include"], str(HOSTPACK_SRC), "-o", str(tmp)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed for {HOSTPACK_SRC.name}:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, HOSTPACK)
+    return HOSTPACK
+
+
 def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
+    build_hostpack(force)
     if not force and up_to_date():
         return LIB
     BUILD.mkdir(exist_ok=True)

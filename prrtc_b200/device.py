@@ -70,26 +70,10 @@ def as_tensor(x, dtype: torch.dtype, device: torch.device, cols: int = 0) -> tor
 def upload(arrays, device: torch.device) -> list[torch.Tensor]:
     """Host arrays -> device tensors through ONE pinned staging buffer and one
     host-to-device copy (each array 256-byte aligned inside it)."""
-    arrays = [np.ascontiguousarray(a) for a in arrays]
-    offs, total = [], 0
-    for a in arrays:
-        offs.append(total)
-        total += (a.nbytes + 255) & ~255
-    total = max(total, 256)
-    host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
-    hv = host.numpy()
-    for a, o in zip(arrays, offs):
-        hv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
-    dev = torch.empty(total, dtype=torch.uint8, device=device)
-    H2D_BYTES[0] += total
-    # torch's caching host allocator records the copy on the stream and keeps
-    # the pinned block out of reuse until that copy has run
-    dev.copy_(host, non_blocking=True)
-    out = []
-    for a, o in zip(arrays, offs):
-        t = dev[o:o + a.nbytes].view(_TORCH_DTYPE[a.dtype.str[1:]]).reshape(a.shape)
-        out.append(t)
-    return out
+    st = Stager(device)
+    keys = [st.add(a, _TORCH_DTYPE[np.asarray(a).dtype.str[1:]]) for a in arrays]
+    st.commit()
+    return [st.get(k) for k in keys]
 
 
 _TORCH_DTYPE = {"f4": torch.float32, "i4": torch.int32, "u1": torch.uint8, "i8": torch.int64, "f8": torch.float64}
@@ -101,12 +85,16 @@ class Stager:
     """Inputs of one call gathered for a single pinned host->device copy.
 
     ``add`` queues a host array (numpy, list, CPU tensor) and returns a key;
-    a tensor already on the device passes through without a copy.  After
-    ``commit`` (one ``upload``), ``get(key)`` is the device tensor."""
+    a tensor already on the device passes through without a copy.
+    ``reserve`` sets aside a region that ``on_fill`` callbacks write straight
+    into the pinned buffer.  After ``commit`` (one host->device copy),
+    ``get(key)`` is the device tensor."""
 
     def __init__(self, device: torch.device):
         self.device = device
-        self._host: list[np.ndarray] = []
+        self._host: list = []  # np.ndarray, or (nbytes, torch dtype, shape) for a reserved region
+        self._fill: list = []
+        self._offsets: list[int] = []
         self._dev: list[torch.Tensor] | None = None
 
     def add(self, x, dtype: torch.dtype, shape=None):
@@ -119,8 +107,42 @@ class Stager:
         self._host.append(np.ascontiguousarray(a))
         return ("h", len(self._host) - 1)
 
+    def reserve(self, dtype: torch.dtype, shape):
+        n = int(np.prod(shape)) * torch.empty((), dtype=dtype).element_size()
+        self._host.append((n, dtype, tuple(shape)))
+        return ("h", len(self._host) - 1)
+
+    def on_fill(self, fn) -> None:
+        """fn(host_bytes: np.ndarray[uint8], offset_of: callable(key) -> int)."""
+        self._fill.append(fn)
+
     def commit(self) -> None:
-        self._dev = upload(self._host, self.device) if self._host else []
+        offs, total = [], 0
+        for a in self._host:
+            offs.append(total)
+            n = a.nbytes if isinstance(a, np.ndarray) else a[0]
+            total += (n + 255) & ~255
+        total = max(total, 256)
+        host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        hv = host.numpy()
+        for a, o in zip(self._host, offs):
+            if isinstance(a, np.ndarray):
+                hv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+        self._offsets = offs
+        for fn in self._fill:
+            fn(hv, lambda key: offs[key[1]])
+        dev = torch.empty(total, dtype=torch.uint8, device=self.device)
+        H2D_BYTES[0] += total
+        # torch's caching host allocator records the copy on the stream and keeps
+        # the pinned block out of reuse until that copy has run
+        dev.copy_(host, non_blocking=True)
+        out = []
+        for a, o in zip(self._host, offs):
+            if isinstance(a, np.ndarray):
+                out.append(dev[o:o + a.nbytes].view(_TORCH_DTYPE[a.dtype.str[1:]]).reshape(a.shape))
+            else:
+                out.append(dev[o:o + a[0]].view(a[1]).reshape(a[2]))
+        self._dev = out
 
     def get(self, key) -> torch.Tensor:
         kind, v = key

@@ -402,6 +402,45 @@ def _shared_table(contexts: Sequence[Optional[dict]], key: str):
     return np.ascontiguousarray(a0, dtype=np.int32 if key == "self_pairs" else np.float32).reshape(-1, _FEAT[key])
 
 
+_PACK_SPECS = tuple((k, f, "i" if dt == np.int32 else "f") for k, f, dt in _TABLES)
+
+
+def _native_pack(contexts: Sequence[Optional[dict]], stage: Stager):
+    """The world / self tables of every context packed by the native host
+    packer straight into the call's pinned staging buffer: padded
+    [B, max_n, feat] tables + int32 counts, or one copy of a table every
+    context shares (same layout as _pack_worlds / _shared_table).  Returns
+    ({key: (table key, counts key or None, width)}, {key: counts}), or None
+    when some table is not a C-contiguous float32 / int32 numpy array (the
+    Python packer then handles the call)."""
+    hp = _lib.hostpack()
+    try:
+        info = hp.scan(contexts, _PACK_SPECS)
+    except TypeError:
+        return None
+    B = len(contexts)
+    world_keys, counts, layout = {}, {}, []
+    for (key, feat, kind), (shared, width, cbytes) in zip(_PACK_SPECS, info):
+        dt = torch.int32 if kind == "i" else torch.float32
+        if shared:
+            rows = int(np.frombuffer(cbytes, np.int32)[0])
+            k_tab = stage.reserve(dt, (rows, feat))
+            world_keys[key] = (k_tab, None, rows)
+            layout.append((True, rows, k_tab, None))
+        else:
+            counts[key] = np.frombuffer(cbytes, np.int32)
+            k_tab, k_cnt = stage.reserve(dt, (B, width, feat)), stage.reserve(torch.int32, (B,))
+            world_keys[key] = (k_tab, k_cnt, width)
+            layout.append((False, width, k_tab, k_cnt))
+
+    def fill(hv, offset_of):
+        hp.fill(contexts, _PACK_SPECS,
+                [(s, w, offset_of(kt), offset_of(kc) if kc is not None else -1) for s, w, kt, kc in layout], hv)
+
+    stage.on_fill(fill)
+    return world_keys, counts
+
+
 _LPT_WEIGHTS = (("world_spheres", 1.0), ("world_capsules", 2.0), ("world_boxes", 3.0), ("world_halfspaces", 1.0))
 
 
@@ -536,7 +575,10 @@ def prrtc_plan_batch_async(
     robot_ctx = DeviceContext(first, dev, world_keys=not per_problem, stager=stage)
     keys = ("world_spheres", "world_capsules", "world_boxes", "world_halfspaces", "self_pairs")
     world_keys, counts = {}, None
-    if per_problem and first is not None:
+    native = _native_pack(contexts, stage) if per_problem and first is not None else None
+    if native is not None:
+        world_keys, counts = native
+    elif per_problem and first is not None:
         # a table every problem shares (typically the robot's self pairs) goes
         # once, unbatched, with no count pointer
         shared = {k: _shared_table(contexts, k) for k in keys}

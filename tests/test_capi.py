@@ -114,3 +114,83 @@ def test_batch_table_sharing_host_logic():
     assert "world_spheres" not in packed
     assert packed["world_boxes"].shape == (3, 3, 15) and counts["world_boxes"].tolist() == [1, 2, 3]
     assert counts["self_pairs"].tolist() == [2, 2, 1]
+
+
+def _native_layout(info, specs, B):
+    """Byte layout of the native packer's output for `info` (scan result)."""
+    layout, off = [], 0
+    for (key, feat, kind), (shared, width, cbytes) in zip(specs, info):
+        if shared:
+            rows = int(np.frombuffer(cbytes, np.int32)[0])
+            layout.append((True, rows, off, -1))
+            off += rows * feat * 4
+        else:
+            layout.append((False, width, off, off + B * width * feat * 4))
+            off += B * width * feat * 4 + B * 4
+    return layout, off
+
+
+def test_native_host_packer_matches_python():
+    """The native packer (scan + fill into a staging buffer) writes exactly the
+    padded tables, counts and shared tables of the Python packer."""
+    from prrtc_b200 import _lib
+    from prrtc_b200.prrtc import _PACK_SPECS, _pack_worlds, _shared_table
+
+    hp = _lib.hostpack()
+    rng = np.random.default_rng(3)
+    sp = rng.integers(0, 50, (40, 2)).astype(np.int32)
+    half = np.array([[0, 0, 1, 0, 0, 0]], np.float32)
+    ctxs = []
+    for i in range(37):
+        c = {"self_pairs": sp if i % 2 else sp.copy(), "world_halfspaces": half.copy(),
+             "world_spheres": rng.normal(size=(int(rng.integers(0, 9)), 4)).astype(np.float32),
+             "world_boxes": rng.normal(size=(int(rng.integers(0, 4)), 15)).astype(np.float32)}
+        if i % 5 == 0:
+            c["world_capsules"] = rng.normal(size=(int(rng.integers(1, 3)), 7)).astype(np.float32)
+        if i == 7:
+            c["world_boxes"] = None
+        ctxs.append(c)
+    ctxs[11] = None
+    B = len(ctxs)
+    for trial in range(2):
+        if trial == 1:  # every context present: self pairs and the halfspace become shared
+            ctxs[11] = dict(ctxs[10])
+        info = hp.scan(ctxs, _PACK_SPECS)
+        layout, total = _native_layout(info, _PACK_SPECS, B)
+        buf = np.full(total + 64, 0x7F, np.uint8)
+        hp.fill(ctxs, _PACK_SPECS, layout, buf)
+        shared = {k: _shared_table(ctxs, k) for k, _, _ in _PACK_SPECS}
+        packed, counts = _pack_worlds(ctxs, B, skip={k for k in shared if shared[k] is not None})
+        for (key, feat, kind), (is_sh, width, cbytes), (_, w2, off, coff) in zip(_PACK_SPECS, info, layout):
+            dt = np.int32 if kind == "i" else np.float32
+            assert is_sh == (shared[key] is not None), key
+            if is_sh:
+                got = buf[off:off + shared[key].nbytes].view(dt).reshape(shared[key].shape)
+                assert np.array_equal(got, shared[key])
+            else:
+                ref = packed[key]
+                assert width == ref.shape[1]
+                got = buf[off:off + ref.nbytes].view(dt).reshape(ref.shape)
+                assert np.array_equal(got, ref), key
+                assert np.array_equal(buf[coff:coff + 4 * B].view(np.int32), counts[key])
+                assert np.array_equal(np.frombuffer(cbytes, np.int32), counts[key])
+        assert (buf[total:] == 0x7F).all()  # nothing written past the layout
+    assert shared["self_pairs"] is not None and shared["world_halfspaces"] is not None
+
+
+def test_native_host_packer_declines_other_types():
+    """Tables that are not C-contiguous float32 / int32 arrays raise TypeError
+    (the batch call then packs in Python); a short staging buffer is refused."""
+    from prrtc_b200 import _lib
+    from prrtc_b200.prrtc import _PACK_SPECS
+
+    hp = _lib.hostpack()
+    good = {"world_spheres": np.zeros((2, 4), np.float32)}
+    for bad in (np.zeros((2, 4), np.float64), [[0.0] * 4] * 2, np.zeros((4, 2), np.float32).T,
+                np.zeros((2, 5), np.float32), np.zeros(8, np.float32)):
+        with pytest.raises(TypeError):
+            hp.scan([good, {"world_spheres": bad}], _PACK_SPECS)
+    info = hp.scan([good, good], _PACK_SPECS)
+    layout, total = _native_layout(info, _PACK_SPECS, 2)
+    with pytest.raises(ValueError):
+        hp.fill([good, good], _PACK_SPECS, layout, np.zeros(max(total - 1, 0), np.uint8))
