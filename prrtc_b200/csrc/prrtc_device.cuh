@@ -764,6 +764,11 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     uint32_t* hw = B.hit + par;
     volatile uint32_t* vhit = hw;
     par ^= 1;
+    // B.hit[2]: next unclaimed work item of this call.  Every thread passed the
+    // previous call's final barrier, and none claims an item before the
+    // barrier after the frames, so thread 0 may reset it here.
+    uint32_t* next_item = B.hit + 2;
+    if (tid == 0) *next_item = 0u;
 
     if (!h.enabled) {
         g.sync();
@@ -774,8 +779,14 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     // range bounds are computed once per chunk.
     const int n_obs = h.Ns + h.Nc + h.Nb + h.Nh;
     const int ctot = world_cost(h);
-    const int n_parts =
-        n_obs == 0 ? 0 : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * h.n_sch)), cdiv(n_obs, 4))));
+    // A full sweep (throughput) takes at most one world item per thread, and
+    // whole-world items once there are more (sphere chunk, waypoint) pairs
+    // than threads: measured faster than finer parts, whose fixed cost per
+    // item outweighs the better spread.  Early-exit checks (latency) take
+    // about two items per thread.
+    const int n_parts = n_obs == 0 ? 0
+                        : full_sweep ? min(kMaxParts, max(1, min(T / max(1, nw * h.n_sch), cdiv(n_obs, 4))))
+                                     : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * h.n_sch)), cdiv(n_obs, 4))));
     // coarse pass: one item = up to 8 coarse spheres of a waypoint over a part
     const int KC = cdiv(K, 8);
     const int n_parts_c =
@@ -891,16 +902,16 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     const int n_world = nw * h.n_sch * n_parts;
     const int n_self = nw * h.n_items;
     const int n_total = n_world + n_self + (sc.pc.n > 0 ? nw * S : 0);
-    for (int it = tid; it < n_total; it += T) {
+    auto run_item = [&](int it) {
         int w;
         bool hit = false;
         if (it < n_world) {
             const int part = it / (nw * h.n_sch), r = it - part * (nw * h.n_sch);
             const int si = r / nw;
             w = r - si * nw;
-            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) continue;
+            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) return;
             const int4 ch = sc.sch[si];
-            if (gated && ch.z >= 0 && !(B.dirty[w * KW + (ch.z >> 5)] & (1u << (ch.z & 31)))) continue;
+            if (gated && ch.z >= 0 && !(B.dirty[w * KW + (ch.z >> 5)] & (1u << (ch.z & 31)))) return;
             float4 s[kSphChunk];
 #pragma unroll
             for (int m = 0; m < kSphChunk; ++m) s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : absent_sphere();
@@ -911,15 +922,15 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
             const int r = it - n_world - n_self;
             const int si = r / nw;
             w = r - si * nw;
-            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) continue;
+            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) return;
             hit = pc_sphere_hits(sc.pc, B.ctr[w * S_pad + si], full_sweep, flops);
         } else {
             const int r = it - n_world;
             const int ii = r / nw;
             w = r - ii * nw;
-            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) continue;
+            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) return;
             const int4 item = sc.item[ii];
-            if (gated && item.w >= 0 && !(B.gate[w * QW + (item.w >> 5)] & (1u << (item.w & 31)))) continue;
+            if (gated && item.w >= 0 && !(B.gate[w * QW + (item.w >> 5)] & (1u << (item.w & 31)))) return;
             const float4* C = &B.ctr[w * S_pad];
             if (item.y >= 0) {  // dense block: spheres [a0, a0+na) x [b0, b0+nb)
                 // self pairs use radius rho = r + inflate/2 per sphere, so the pair
@@ -968,6 +979,23 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         const unsigned active = __activemask();
         const unsigned bits = __reduce_or_sync(active, hit ? (1u << w) : 0u);
         if (bits && (threadIdx.x & 31) == (__ffs(active) - 1)) atomicOr(hw, bits);
+    };
+    if (G::kWarp) {
+        for (int it = tid; it < n_total; it += T) run_item(it);
+    } else {
+        // Items are claimed by warps, 32 consecutive items at a time, from a
+        // shared counter: warps whose items were cheap (or skipped) take more,
+        // so no warp idles at the closing barrier while items remain.  Item
+        // order (world items first, waypoint fastest) keeps a warp's lanes on
+        // the same obstacles.
+        const int lane = tid & 31;
+        for (;;) {
+            int base = 0;
+            if (lane == 0) base = (int)atomicAdd(next_item, 32u);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n_total) break;
+            if (base + lane < n_total) run_item(base + lane);
+        }
     }
     if (B.stats) {
         if (tid == 0) {
