@@ -65,8 +65,8 @@ def parse():
     ap.add_argument("--tune", choices=["joint", "bucket"], default="bucket",
                     help="explorer counts tuned per bucket alone (default; measured 144 K vs 139-143 K plans/s) "
                          "or with the buckets running together (joint)")
-    ap.add_argument("--kernel", choices=["cc", "nn"], default=None,
-                    help="run only the standalone FK+collision (cc) or nearest-neighbour (nn) measurement")
+    ap.add_argument("--kernel", choices=["cc", "nn", "smooth"], default=None,
+                    help="run only the standalone FK+collision (cc), nearest-neighbour (nn) or smoothing adjoint (smooth) measurement")
     return ap.parse_args()
 
 
@@ -535,6 +535,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
 
     out.update(measure_cc(torch, dev, fp32))
     out.update(measure_nn(torch, dev, peaks))
+    out.update(measure_smooth(torch, dev))
 
     # --- CPU baseline (the reference's host loop restated), 1 core, bounded sample
     from oracle import oracle as O
@@ -581,6 +582,43 @@ def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
                                       "flat checker, full sweep", "checks_per_s": n / (best * 1e-3),
                           "flops_per_check": f_cfg, "achieved_tflops": ach,
                           "frac_of_fp32_peak": (ach / fp32) if fp32 else None}}
+
+
+def measure_smooth(torch, dev, paths: int = 512, waypoints: int = 64, launches: int = 20, reps: int = 3):
+    """Smoothing adjoint (prrtc_b200_smooth_cost_grad: cost and gradient of the
+    smooth collision + length cost through FK, link transforms recomputed in
+    the backward sweep) on the tabletop scene: `paths` paths of `waypoints`
+    waypoints, one gradient evaluation per launch (one smoothing step)."""
+    from prrtc_b200 import scenes
+    from prrtc_b200.context import build_collision_context
+    from prrtc_b200.smoothing import SmoothContext
+
+    rng = np.random.default_rng(1)
+    ctx = build_collision_context(scenes.arm(0), scenes.tabletop_world(rng))
+    sctx = SmoothContext(ctx, 7, device=dev)
+    a = rng.uniform(-2.8, 2.8, (paths, 1, 7))
+    b = rng.uniform(-2.8, 2.8, (paths, 1, 7))
+    t = np.linspace(0.0, 1.0, waypoints)[None, :, None]
+    wp = torch.from_numpy((a + (b - a) * t).astype(np.float32)).to(dev)
+    sctx.cost_grad(wp)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(launches):
+            sctx.cost_grad(wp)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / launches)
+    S, P = 56, 960
+    pairs = S * (32 + 8 + 20 + 1) + P  # robot-sphere / primitive pairs + self pairs per waypoint
+    n = paths * waypoints
+    return {"smooth_adjoint": {"workload": f"tabletop scene, {paths} paths x {waypoints} waypoints x 7 dims, cost + "
+                                          "gradient per launch", "ms_per_launch": best,
+                               "waypoint_gradients_per_s": n / (best * 1e-3),
+                               "pair_terms_per_s": n * pairs / (best * 1e-3),
+                               "pairs_per_waypoint": pairs}}
 
 
 def measure_nn(torch, dev, peaks, reps: int = 3, launches: int = 20):
@@ -652,6 +690,8 @@ def run_kernel(a):
     lib = _lib.load()
     if a.kernel == "cc":
         out = measure_cc(torch, dev, fp32_peak_tflops(torch, lib, dev))
+    elif a.kernel == "smooth":
+        out = measure_smooth(torch, dev)
     else:
         out = measure_nn(torch, dev, measured_peaks())
     print(json.dumps(out))

@@ -25,12 +25,12 @@
 
 namespace prrtc {
 
-__device__ __forceinline__ float softplus_b(float x, float beta) {
-    const float z = beta * x;
-    return (z > 0.0f ? z + log1pf(expf(-z)) : log1pf(expf(z))) / beta;
-}
-
-__device__ __forceinline__ float sigmoid_f(float z) { return 1.0f / (1.0f + expf(-z)); }
+// softplus_beta(x) and sigmoid(beta x) from one exponential: with z = beta x
+// and e = exp(-|z|), softplus_beta = (max(z, 0) + log1p(e)) / beta and
+// sigmoid = 1/(1+e) for z >= 0, e/(1+e) otherwise.  A pair with z < kTailZ
+// adds less than exp(kTailZ)/beta (below 1e-15 for beta >= 1) to the cost
+// and to every gradient entry, and is skipped.
+constexpr float kTailZ = -34.0f;
 
 struct SmoothArgs {
     const unsigned char* blob;
@@ -48,11 +48,25 @@ __host__ __device__ inline int smooth_warp_floats(int J, int S) {
     return (J * 12 + S * 4 + S * 4 + J * 8 + J + kDimMax + 3) & ~3;  // keep every warp slice 16-byte aligned
 }
 
-// accumulate the pair term for distance d with gradient direction u (dd/dc = u)
-__device__ __forceinline__ void pair_term(float d, float margin, float beta, float& cost, float& sig) {
-    const float x = margin - d;
-    cost += softplus_b(x, beta);
-    sig = sigmoid_f(beta * x);
+// Accumulate the cost term of a pair at distance d.  sig = sigmoid(beta
+// (margin - d)) is the factor of -dd/dc in the gradient (0 for a skipped pair).
+__device__ __forceinline__ void pair_term(float d, float margin, float beta, float inv_beta, float& cost,
+                                          float& sig) {
+    const float z = beta * (margin - d);
+    if (!(z >= kTailZ)) {  // far pair (or NaN distance): no contribution
+        sig = 0.0f;
+        return;
+    }
+    const float e = expf(-fabsf(z));
+    cost = fmaf(fmaxf(z, 0.0f) + log1pf(e), inv_beta, cost);
+    const float r = __fdividef(1.0f, 1.0f + e);
+    sig = z >= 0.0f ? r : e * r;
+}
+
+// |v| and 1/|v| (0 and 0 for v = 0) from one reciprocal square root
+__device__ __forceinline__ void norm_rnorm(float d2, float& n, float& rn) {
+    rn = d2 > 0.0f ? rsqrtf(d2) : 0.0f;
+    n = d2 * rn;
 }
 
 template <int WARPS>
@@ -98,6 +112,7 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
     __syncwarp();
     // 2a. world pairs: one sphere per lane
     float cost = 0.0f;
+    const float inv_beta = 1.0f / a.beta;
     for (int s = lane; s < S; s += 32) {
         if (sc.sfr[s] < 0) continue;
         const float4 cs = ctr[s];
@@ -107,10 +122,10 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
             const float4 o1 = sc.ws[2 * o + 1];
             const float4 ob = make_float4(o1.x, o1.y, o1.z, -0.5f * sc.ws[2 * o].w);
             const float dx = cs.x - ob.x, dy = cs.y - ob.y, dz = cs.z - ob.z;
-            const float n = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-            float sig;
-            pair_term(n - r - ob.w, a.margin, a.beta, cost, sig);
-            const float k = n > 0.0f ? -sig / n : 0.0f;
+            float n, rn, sig;
+            norm_rnorm(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), n, rn);
+            pair_term(n - r - ob.w, a.margin, a.beta, inv_beta, cost, sig);
+            const float k = -sig * rn;
             gx = fmaf(k, dx, gx); gy = fmaf(k, dy, gy); gz = fmaf(k, dz, gz);
         }
         for (int o = 0; o < h.Nc; ++o) {
@@ -118,10 +133,10 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
             const float wx = cs.x - p1.x, wy = cs.y - p1.y, wz = cs.z - p1.z;
             const float t = __saturatef(fmaf(dp.x, cs.x, fmaf(dp.y, cs.y, fmaf(dp.z, cs.z, dp.w))));
             const float ex = fmaf(-t, dl.x, wx), ey = fmaf(-t, dl.y, wy), ez = fmaf(-t, dl.z, wz);
-            const float n = sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
-            float sig;
-            pair_term(n - r - p1.w, a.margin, a.beta, cost, sig);
-            const float k = n > 0.0f ? -sig / n : 0.0f;
+            float n, rn, sig;
+            norm_rnorm(fmaf(ex, ex, fmaf(ey, ey, ez * ez)), n, rn);
+            pair_term(n - r - p1.w, a.margin, a.beta, inv_beta, cost, sig);
+            const float k = -sig * rn;
             gx = fmaf(k, ex, gx); gy = fmaf(k, ey, gy); gz = fmaf(k, ez, gz);
         }
         for (int o = 0; o < h.Nb; ++o) {
@@ -144,12 +159,13 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
             }
             float d, ddx = 0.0f, ddy = 0.0f, ddz = 0.0f;
             if (out2 > 0.0f) {
-                const float n = sqrtf(out2);
+                float n, rn;
+                norm_rnorm(out2, n, rn);
                 d = n - r;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     if (qv[k] > 0.0f) {
-                        const float coef = copysignf(qv[k] / n, l[k]);
+                        const float coef = copysignf(qv[k] * rn, l[k]);
                         ddx = fmaf(coef, ax[k].x, ddx); ddy = fmaf(coef, ax[k].y, ddy); ddz = fmaf(coef, ax[k].z, ddz);
                     }
                 }
@@ -159,14 +175,14 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
                 ddx = sgn * ax[kmax].x; ddy = sgn * ax[kmax].y; ddz = sgn * ax[kmax].z;
             }
             float sig;
-            pair_term(d, a.margin, a.beta, cost, sig);
+            pair_term(d, a.margin, a.beta, inv_beta, cost, sig);
             gx = fmaf(-sig, ddx, gx); gy = fmaf(-sig, ddy, gy); gz = fmaf(-sig, ddz, gz);
         }
         for (int o = 0; o < h.Nh; ++o) {
             const float4 hs = sc.wh[o];
             const float d = fmaf(hs.x, cs.x, fmaf(hs.y, cs.y, fmaf(hs.z, cs.z, hs.w))) - r;
             float sig;
-            pair_term(d, a.margin, a.beta, cost, sig);
+            pair_term(d, a.margin, a.beta, inv_beta, cost, sig);
             gx = fmaf(-sig, hs.x, gx); gy = fmaf(-sig, hs.y, gy); gz = fmaf(-sig, hs.z, gz);
         }
         g[s] = make_float4(gx, gy, gz, 0.0f);
@@ -179,10 +195,11 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
         if (sc.sfr[pr.x] < 0 || sc.sfr[pr.y] < 0) continue;
         const float4 ci = ctr[pr.x], cj = ctr[pr.y];
         const float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
-        const float n = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-        float sig;
-        pair_term(n - ci.w - cj.w, a.margin, a.beta, cost, sig);
-        const float kk = n > 0.0f ? -sig / n : 0.0f;
+        float n, rn, sig;
+        norm_rnorm(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), n, rn);
+        pair_term(n - ci.w - cj.w, a.margin, a.beta, inv_beta, cost, sig);
+        if (sig == 0.0f) continue;  // nothing to add
+        const float kk = -sig * rn;
         atomicAdd(&g[pr.x].x, kk * dx); atomicAdd(&g[pr.x].y, kk * dy); atomicAdd(&g[pr.x].z, kk * dz);
         atomicAdd(&g[pr.y].x, -kk * dx); atomicAdd(&g[pr.y].y, -kk * dy); atomicAdd(&g[pr.y].z, -kk * dz);
     }
