@@ -27,10 +27,28 @@ namespace prrtc {
 
 // softplus_beta(x) and sigmoid(beta x) from one exponential: with z = beta x
 // and e = exp(-|z|), softplus_beta = (max(z, 0) + log1p(e)) / beta and
-// sigmoid = 1/(1+e) for z >= 0, e/(1+e) otherwise.  A pair with z < kTailZ
-// adds less than exp(kTailZ)/beta (below 1e-15 for beta >= 1) to the cost
-// and to every gradient entry, and is skipped.
+// sigmoid = 1/(1+e) for z >= 0, e/(1+e) otherwise.  Below z = kTailZ a pair
+// adds less than exp(kTailZ)/beta (below 1e-15 for beta >= 1) to the cost and
+// to every gradient entry; its sigmoid is reported as 0 so that callers can
+// skip the gradient scatter.
 constexpr float kTailZ = -34.0f;
+
+// log1p(e) for e in [0, 1] without branches: log1p(e) = 2 atanh(s) with
+// s = e / (2 + e) in [0, 1/3], and atanh(s) = s + s^3/3 + s^5/5 + ... summed
+// to s^15 (the first omitted term is below 1.5e-9 of the sum for s <= 1/3).
+__device__ __forceinline__ float log1p_unit(float e) {
+    const float s = __fdividef(e, 2.0f + e);
+    const float s2 = s * s;
+    float p = 1.0f / 15.0f;
+    p = fmaf(p, s2, 1.0f / 13.0f);
+    p = fmaf(p, s2, 1.0f / 11.0f);
+    p = fmaf(p, s2, 1.0f / 9.0f);
+    p = fmaf(p, s2, 1.0f / 7.0f);
+    p = fmaf(p, s2, 1.0f / 5.0f);
+    p = fmaf(p, s2, 1.0f / 3.0f);
+    p = fmaf(p, s2, 1.0f);
+    return 2.0f * s * p;
+}
 
 struct SmoothArgs {
     const unsigned char* blob;
@@ -53,14 +71,10 @@ __host__ __device__ inline int smooth_warp_floats(int J, int S) {
 __device__ __forceinline__ void pair_term(float d, float margin, float beta, float inv_beta, float& cost,
                                           float& sig) {
     const float z = beta * (margin - d);
-    if (!(z >= kTailZ)) {  // far pair (or NaN distance): no contribution
-        sig = 0.0f;
-        return;
-    }
-    const float e = expf(-fabsf(z));
-    cost = fmaf(fmaxf(z, 0.0f) + log1pf(e), inv_beta, cost);
+    const float e = __expf(-fabsf(z));
+    cost = fmaf(fmaxf(z, 0.0f) + log1p_unit(e), inv_beta, cost);
     const float r = __fdividef(1.0f, 1.0f + e);
-    sig = z >= 0.0f ? r : e * r;
+    sig = z >= kTailZ ? (z >= 0.0f ? r : e * r) : 0.0f;
 }
 
 // |v| and 1/|v| (0 and 0 for v = 0) from one reciprocal square root
@@ -148,32 +162,29 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
             float4 hl = sc.wb[4 * o + 3];
             hl = make_float4(hl.x * kBoxScale, hl.y * kBoxScale, hl.z * kBoxScale, 0.0f);
             const float hh[3] = {hl.x, hl.y, hl.z};
-            float l[3], qv[3], out2 = 0.0f, qmax = -INFINITY;
-            int kmax = 0;
+            // signed distance to the box without branches: outside, |max(q, 0)|
+            // with gradient sum_k sign(l_k) max(q_k, 0)/n a_k; inside, the
+            // largest q_k (first axis on ties) with gradient sign(l_k) a_k
+            float l[3], qv[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 l[k] = fmaf(ax[k].x, cs.x, fmaf(ax[k].y, cs.y, fmaf(ax[k].z, cs.z, ax[k].w)));
                 qv[k] = fabsf(l[k]) - hh[k];
-                if (qv[k] > 0.0f) out2 = fmaf(qv[k], qv[k], out2);
-                if (qv[k] > qmax) { qmax = qv[k]; kmax = k; }
             }
-            float d, ddx = 0.0f, ddy = 0.0f, ddz = 0.0f;
-            if (out2 > 0.0f) {
-                float n, rn;
-                norm_rnorm(out2, n, rn);
-                d = n - r;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    if (qv[k] > 0.0f) {
-                        const float coef = copysignf(qv[k] * rn, l[k]);
-                        ddx = fmaf(coef, ax[k].x, ddx); ddy = fmaf(coef, ax[k].y, ddy); ddz = fmaf(coef, ax[k].z, ddz);
-                    }
-                }
-            } else {
-                d = qmax - r;
-                const float sgn = copysignf(1.0f, l[kmax]);
-                ddx = sgn * ax[kmax].x; ddy = sgn * ax[kmax].y; ddz = sgn * ax[kmax].z;
-            }
+            const float p0 = fmaxf(qv[0], 0.0f), p1 = fmaxf(qv[1], 0.0f), p2 = fmaxf(qv[2], 0.0f);
+            const float out2 = fmaf(p0, p0, fmaf(p1, p1, p2 * p2));
+            float n, rn;
+            norm_rnorm(out2, n, rn);
+            const float qmax = fmaxf(qv[0], fmaxf(qv[1], qv[2]));
+            const bool outside = out2 > 0.0f;
+            const float d = (outside ? n : qmax) - r;
+            const bool k0 = qv[0] == qmax, k1 = !k0 && qv[1] == qmax, k2 = !k0 && !k1;
+            const float c0 = copysignf(outside ? p0 * rn : (k0 ? 1.0f : 0.0f), l[0]);
+            const float c1 = copysignf(outside ? p1 * rn : (k1 ? 1.0f : 0.0f), l[1]);
+            const float c2 = copysignf(outside ? p2 * rn : (k2 ? 1.0f : 0.0f), l[2]);
+            const float ddx = fmaf(c0, ax[0].x, fmaf(c1, ax[1].x, c2 * ax[2].x));
+            const float ddy = fmaf(c0, ax[0].y, fmaf(c1, ax[1].y, c2 * ax[2].y));
+            const float ddz = fmaf(c0, ax[0].z, fmaf(c1, ax[1].z, c2 * ax[2].z));
             float sig;
             pair_term(d, a.margin, a.beta, inv_beta, cost, sig);
             gx = fmaf(-sig, ddx, gx); gy = fmaf(-sig, ddy, gy); gz = fmaf(-sig, ddz, gz);
