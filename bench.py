@@ -510,27 +510,35 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
                          "copied to the host)"}
 
     # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    solved_plain = 0
     from prrtc_b200.batch import bucket_problems
 
-    for N, ps in bucket_problems(problems).items():
-        G = max(p.goals.shape[0] for p in ps)
-        goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
-        for i, p in enumerate(ps):
-            goals[i, : p.goals.shape[0]] = p.goals
-        res = prrtc_plan_batch(np.stack([p.start for p in ps]), goals, max_iterations=settings.max_iterations,
-                               num_new_samples=128, max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper,
-                               collision_context=[p.context for p in ps], collision_checker=settings.collision_checker,
-                               goal_counts=[p.goals.shape[0] for p in ps], edge_resolution=settings.edge_resolution,
-                               launch="per_problem", return_trees=False)
-        solved_plain += sum(r.solved for r in res)
+    def plain(ps_all):
+        solved = 0
+        for N, ps in bucket_problems(ps_all).items():
+            G = max(p.goals.shape[0] for p in ps)
+            goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
+            for i, p in enumerate(ps):
+                goals[i, : p.goals.shape[0]] = p.goals
+            res = prrtc_plan_batch(np.stack([p.start for p in ps]), goals, max_iterations=settings.max_iterations,
+                                   num_new_samples=128, max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper,
+                                   collision_context=[p.context for p in ps],
+                                   collision_checker=settings.collision_checker,
+                                   goal_counts=[p.goals.shape[0] for p in ps],
+                                   edge_resolution=settings.edge_resolution, launch="per_problem",
+                                   return_trees=False)
+            solved += sum(r.solved for r in res)
+        return solved
+
+    plain(problems)  # warm: first-call stream and workspace set-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    solved_plain = plain(problems)
     torch.cuda.synchronize()
     dtp = time.perf_counter() - t0
     out["plain_per_problem"] = {"plans_per_s": solved_plain / dtp, "success_rate": solved_plain / len(problems),
                                 "note": "one plain planner launch per problem over 8 streams, 128 explorers each, "
-                                        "host-timed incl. per-problem set-up (the reference's batch form)"}
+                                        "host-timed incl. per-problem set-up (the reference's batch form); "
+                                        "second of two passes"}
     out["batched_vs_plain"] = line["value"] / max(out["plain_per_problem"]["plans_per_s"], 1e-9)
 
     out.update(measure_cc(torch, dev, fp32))

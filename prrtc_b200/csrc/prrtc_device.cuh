@@ -764,11 +764,6 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     uint32_t* hw = B.hit + par;
     volatile uint32_t* vhit = hw;
     par ^= 1;
-    // B.hit[2]: next unclaimed work item of this call.  Every thread passed the
-    // previous call's final barrier, and none claims an item before the
-    // barrier after the frames, so thread 0 may reset it here.
-    uint32_t* next_item = B.hit + 2;
-    if (tid == 0) *next_item = 0u;
 
     if (!h.enabled) {
         g.sync();
@@ -980,23 +975,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         const unsigned bits = __reduce_or_sync(active, hit ? (1u << w) : 0u);
         if (bits && (threadIdx.x & 31) == (__ffs(active) - 1)) atomicOr(hw, bits);
     };
-    if (G::kWarp) {
-        for (int it = tid; it < n_total; it += T) run_item(it);
-    } else {
-        // Items are claimed by warps, 32 consecutive items at a time, from a
-        // shared counter: warps whose items were cheap (or skipped) take more,
-        // so no warp idles at the closing barrier while items remain.  Item
-        // order (world items first, waypoint fastest) keeps a warp's lanes on
-        // the same obstacles.
-        const int lane = tid & 31;
-        for (;;) {
-            int base = 0;
-            if (lane == 0) base = (int)atomicAdd(next_item, 32u);
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (base >= n_total) break;
-            if (base + lane < n_total) run_item(base + lane);
-        }
-    }
+    for (int it = tid; it < n_total; it += T) run_item(it);
     if (B.stats) {
         if (tid == 0) {
             unsigned long long fk = (unsigned long long)nw * (J * (kFlopJointLocal + kFlopJointChain) + S * kFlopXform);
