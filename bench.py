@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--tune", choices=["joint", "bucket"], default="bucket",
                     help="explorer counts tuned per bucket alone (default; measured 144 K vs 139-143 K plans/s) "
                          "or with the buckets running together (joint)")
+    ap.add_argument("--tuning", default=None, metavar="E,T,CW",
+                    help="skip the autotuner: explorers per problem, threads per explorer, waypoints per chunk")
     ap.add_argument("--kernel", choices=["cc", "nn", "smooth"], default=None,
                     help="run only the standalone FK+collision (cc), nearest-neighbour (nn) or smoothing adjoint (smooth) measurement")
     return ap.parse_args()
@@ -293,7 +295,11 @@ def run_ours(a):
     else:
         groups = dict(buckets)
         cap_of = {N: N for N in buckets}
-    tuned = {k: choose(ps, cap_of[k], settings, dev) for k, ps in groups.items()}
+    if a.tuning:
+        e_, t_, c_ = (int(x) for x in a.tuning.split(","))
+        tuned = {k: {"num_new_samples": e_, "threads_per_explorer": t_, "waypoint_chunk": c_} for k in groups}
+    else:
+        tuned = {k: choose(ps, cap_of[k], settings, dev) for k, ps in groups.items()}
     # optional: settle the explorer counts with the buckets running together
     if a.tune == "joint" and a.launch == "buckets":
         tuned = choose_joint(buckets, tuned, settings, dev)

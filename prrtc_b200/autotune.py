@@ -3,9 +3,9 @@
 For one capacity bucket, times a plan of the bucket's problems for each
 candidate (explorers per problem = samples per iteration, threads per explorer
 -- 32 meaning one explorer per warp, four per CTA --, waypoints per
-shared-memory chunk) and keeps the fastest by solved plans
-per second (median of three launches); a candidate must beat the incumbent by
-3% to replace it.  Results
+shared-memory chunk) by solved plans per second: the median of three launches
+per candidate, then a second round between the three best (six more launches
+each, taken in turn) decides.  Results
 are cached per (device, bucket, problem count, shape) in
 ``~/.cache/prrtc_b200/autotune.json``.
 """
@@ -41,36 +41,60 @@ def _load() -> dict:
         return {}
 
 
-def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = True) -> dict:
+def _rate(pl) -> float:
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    pl.launch()
+    e1.record()
+    e1.synchronize()
+    solved = int((pl.summary_block()[:, 8] == 1).sum().item())
+    return solved / (e0.elapsed_time(e1) * 1e-3)
+
+
+def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = True, finalists: int = 3,
+           final_reps: int = 6) -> dict:
     """Best {num_new_samples, threads_per_explorer, waypoint_chunk} for this bucket
-    (N: one tree capacity, or a per-problem list of them)."""
+    (N: one tree capacity, or a per-problem list of them).
+
+    Two rounds: every candidate is timed by the median of three launches (the
+    explorers race, so one launch is noisy); the best ``finalists`` are then
+    timed again, ``final_reps`` launches each in turn (so that clock or
+    thermal drift hits them alike), and the best median over all their
+    launches wins."""
     from .batch import BatchPlanner, PlanSettings
 
-    key = "v5|" + _key(dev, N, problems, settings)
+    key = "v6|" + _key(dev, N, problems, settings)
     cache = _load() if use_cache else {}
     if key in cache:
         return dict(cache[key])
-    best, best_rate = candidates[0], -1.0
-    for E, T, CW in candidates:
+
+    def planner(c):
+        E, T, CW = c
         s = PlanSettings(**{**settings.__dict__, "num_new_samples": E, "threads_per_explorer": T,
                             "waypoint_chunk": CW})
-        pl = BatchPlanner(problems, N, s, dev)
+        return BatchPlanner(problems, N, s, dev)
+
+    def med(r):
+        return sorted(r)[len(r) // 2]
+
+    rates = {}
+    for c in candidates:
+        pl = planner(c)
         pl.launch()  # warm
         torch.cuda.synchronize(dev)
-        # median of three launches: the explorers race, so one launch is noisy
-        rates = []
-        for _ in range(3):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            pl.launch()
-            e1.record()
-            e1.synchronize()
-            solved = int((pl.summary_block()[:, 8] == 1).sum().item())
-            rates.append(solved / (e0.elapsed_time(e1) * 1e-3))
-        rate = sorted(rates)[1]
-        if rate > best_rate * 1.03:
-            best, best_rate = (E, T, CW), rate
+        rates[c] = [_rate(pl) for _ in range(3)]
         del pl
+    top = sorted(candidates, key=lambda c: -med(rates[c]))[:max(1, finalists)]
+    if len(top) > 1:
+        pls = {c: planner(c) for c in top}
+        for pl in pls.values():
+            pl.launch()
+        torch.cuda.synchronize(dev)
+        for _ in range(final_reps):
+            for c in top:
+                rates[c].append(_rate(pls[c]))
+        del pls
+    best = max(top, key=lambda c: med(rates[c]))
     best = {"num_new_samples": best[0], "threads_per_explorer": best[1], "waypoint_chunk": best[2]}
     if use_cache:
         cache[key] = best
