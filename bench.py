@@ -65,8 +65,9 @@ def parse():
     ap.add_argument("--tune", choices=["joint", "bucket"], default="bucket",
                     help="explorer counts tuned per bucket alone (default; measured 144 K vs 139-143 K plans/s) "
                          "or with the buckets running together (joint)")
-    ap.add_argument("--tuning", default=None, metavar="E,T,CW",
-                    help="skip the autotuner: explorers per problem, threads per explorer, waypoints per chunk")
+    ap.add_argument("--tuning", default=None, metavar="E,T,CW[,R]",
+                    help="skip the autotuner: explorers per problem, threads per explorer, waypoints per chunk, "
+                         "CTAs per SM (0: as many as fit)")
     ap.add_argument("--kernel", choices=["cc", "nn", "smooth"], default=None,
                     help="run only the standalone FK+collision (cc), nearest-neighbour (nn) or smoothing adjoint (smooth) measurement")
     return ap.parse_args()
@@ -296,8 +297,9 @@ def run_ours(a):
         groups = dict(buckets)
         cap_of = {N: N for N in buckets}
     if a.tuning:
-        e_, t_, c_ = (int(x) for x in a.tuning.split(","))
-        tuned = {k: {"num_new_samples": e_, "threads_per_explorer": t_, "waypoint_chunk": c_} for k in groups}
+        v_ = [int(x) for x in a.tuning.split(",")] + [0]
+        tuned = {k: {"num_new_samples": v_[0], "threads_per_explorer": v_[1], "waypoint_chunk": v_[2],
+                     "ctas_per_sm": v_[3]} for k in groups}
     else:
         tuned = {k: choose(ps, cap_of[k], settings, dev) for k, ps in groups.items()}
     # optional: settle the explorer counts with the buckets running together
@@ -479,8 +481,8 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
                     max_nodes=cap, min_vals=ps[0].lower, max_vals=ps[0].upper, collision_context=ctxs,
                     collision_checker=settings.collision_checker, goal_counts=gcounts,
                     edge_resolution=settings.edge_resolution,
-                    threads_per_explorer=tuned[key]["threads_per_explorer"], return_trees=False,
-                    paths_on_host=True)))
+                    threads_per_explorer=tuned[key]["threads_per_explorer"],
+                    ctas_per_sm=tuned[key].get("ctas_per_sm", 0), return_trees=False, paths_on_host=True)))
         return pending
 
     def collect(pending):

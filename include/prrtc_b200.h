@@ -171,6 +171,10 @@ typedef struct {
                                     problem: 0 = default (about 4 million), > 0 = that many,
                                     < 0 = none (the wait gives up at once: tests the failure
                                     path without a fault) */
+    int32_t ctas_per_sm;         /* batched planner: > 0 = at most that many CTAs per SM, with the
+                                    shared-memory carve-out that just holds them, so the rest of
+                                    the SM's unified L1 / shared memory serves as L1 for the
+                                    trees, radii and scenes; 0 = as many as fit (default) */
 } prrtc_tuning_t;
 
 size_t prrtc_b200_plan_workspace_size(const prrtc_inputs_t* in, const prrtc_attrs_t* attrs,

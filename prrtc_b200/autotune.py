@@ -3,7 +3,7 @@
 For one capacity bucket, times a plan of the bucket's problems for each
 candidate (explorers per problem = samples per iteration, threads per explorer
 -- 32 meaning one explorer per warp, four per CTA --, waypoints per
-shared-memory chunk) by solved plans per second: the median of three launches
+shared-memory chunk, CTAs per SM) by solved plans per second: the median of three launches
 per candidate, then a second round between the three best (six more launches
 each, taken in turn) decides.  Results
 are cached per (device, bucket, problem count, shape) in
@@ -20,7 +20,8 @@ import torch
 SAMPLES = (1, 2, 4, 8, 16)
 THREADS = (64, 128)  # 32 (one explorer per warp) stays available but lost on every bucket measured
 CHUNKS = (8, 16, 32)
-CANDIDATES = tuple((e, t, c) for t in THREADS for c in CHUNKS for e in SAMPLES)
+CTAS_PER_SM = (0, 2)  # 0: as many as fit; 2: two, with the rest of shared memory given to L1
+CANDIDATES = tuple((e, t, c, r) for r in CTAS_PER_SM for t in THREADS for c in CHUNKS for e in SAMPLES)
 CACHE = Path(os.environ.get("PRRTC_B200_CACHE", Path.home() / ".cache" / "prrtc_b200")) / "autotune.json"
 
 
@@ -53,7 +54,7 @@ def _rate(pl) -> float:
 
 def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = True, finalists: int = 3,
            final_reps: int = 6) -> dict:
-    """Best {num_new_samples, threads_per_explorer, waypoint_chunk} for this bucket
+    """Best {num_new_samples, threads_per_explorer, waypoint_chunk, ctas_per_sm} for this bucket
     (N: one tree capacity, or a per-problem list of them).
 
     Two rounds: every candidate is timed by the median of three launches (the
@@ -63,15 +64,15 @@ def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = 
     launches wins."""
     from .batch import BatchPlanner, PlanSettings
 
-    key = "v6|" + _key(dev, N, problems, settings)
+    key = "v7|" + _key(dev, N, problems, settings)
     cache = _load() if use_cache else {}
     if key in cache:
         return dict(cache[key])
 
     def planner(c):
-        E, T, CW = c
+        E, T, CW, R = c
         s = PlanSettings(**{**settings.__dict__, "num_new_samples": E, "threads_per_explorer": T,
-                            "waypoint_chunk": CW})
+                            "waypoint_chunk": CW, "ctas_per_sm": R})
         return BatchPlanner(problems, N, s, dev)
 
     def med(r):
@@ -95,7 +96,8 @@ def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = 
                 rates[c].append(_rate(pls[c]))
         del pls
     best = max(top, key=lambda c: med(rates[c]))
-    best = {"num_new_samples": best[0], "threads_per_explorer": best[1], "waypoint_chunk": best[2]}
+    best = {"num_new_samples": best[0], "threads_per_explorer": best[1], "waypoint_chunk": best[2],
+            "ctas_per_sm": best[3]}
     if use_cache:
         cache[key] = best
         try:

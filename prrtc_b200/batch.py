@@ -39,6 +39,7 @@ class PlanSettings:
     waypoint_chunk: int = 16
     resident_ctas: int = 0
     tail_explorers: bool = True
+    ctas_per_sm: int = 0
 
 
 class BatchPlanner:
@@ -106,7 +107,7 @@ class BatchPlanner:
                             s.dynamic_domain, s.dd_alpha, s.dd_radius, s.dd_min_radius, dim, self.N, s.granularity,
                             _resolve_collision_mode(s.collision_checker), s.collision_margin)
         self.tun = _tuning(s.edge_resolution, s.threads_per_explorer, s.waypoint_chunk, s.resident_ctas,
-                           s.tail_explorers)
+                           s.tail_explorers, s.ctas_per_sm)
         self.stats = torch.zeros(4, dtype=torch.int64, device=self.dev) if stats else None
         if self.stats is not None:
             self.tun.stats = self.stats.data_ptr()

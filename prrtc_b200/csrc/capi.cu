@@ -87,6 +87,7 @@ struct Tuned {
     const prrtc_point_cloud_t* cloud;
     int tail_join;
     int wait_polls;
+    int ctas_per_sm;
 };
 
 static PcView pc_view(const prrtc_point_cloud_t* c) {
@@ -105,7 +106,7 @@ static bool cloud_ok(const prrtc_point_cloud_t* c) {
 }
 
 static Tuned tuned(const prrtc_tuning_t* t) {
-    Tuned o{0.0f, 128, 16, 0, nullptr, nullptr, 1, 0};
+    Tuned o{0.0f, 128, 16, 0, nullptr, nullptr, 1, 0, 0};
     if (t) {
         if (t->edge_resolution > 0.0f) o.edge_res = t->edge_resolution;
         if (t->threads_per_explorer == 32 || t->threads_per_explorer == 64 || t->threads_per_explorer == 128 ||
@@ -117,6 +118,7 @@ static Tuned tuned(const prrtc_tuning_t* t) {
         o.cloud = t->point_cloud;
         o.tail_join = t->tail_explorers < 0 ? 0 : 1;
         o.wait_polls = t->staging_wait_polls > 0 ? t->staging_wait_polls : (t->staging_wait_polls < 0 ? -1 : 0);
+        o.ctas_per_sm = t->ctas_per_sm > 0 ? t->ctas_per_sm : 0;
     }
     return o;
 }
@@ -138,6 +140,7 @@ static void fill_launch(PlanLaunch& L, const prrtc_outputs_t* out, const prrtc_a
     L.pc = pc_view(tu.cloud);
     L.tail_join = tu.tail_join;
     L.wait_polls = tu.wait_polls;
+    L.ctas_per_sm = tu.ctas_per_sm;
 }
 
 static bool outputs_ok(const prrtc_outputs_t* o) {

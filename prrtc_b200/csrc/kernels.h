@@ -74,6 +74,7 @@ struct PlanLaunch {
     int warp_explorers;                // persistent form with 32 threads: one explorer per warp (4 per CTA)
     int tail_join;                     // persistent form: idle CTAs join running problems as extra explorers
     int wait_polls;                    // polls of the scene-staging wait before it gives up (0: default, <0: none)
+    int ctas_per_sm;                   // persistent form: > 0 caps CTAs per SM and sizes the shared-memory carve-out
     unsigned long long* stats;         // optional device counters (kStat*)
     PcView pc;                         // environment point cloud shared by every problem (pc.n = 0: none)
 };

@@ -908,10 +908,30 @@ cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
     const int threads = warps ? kWarpsPerCta * 32 : L.threads;
     if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) != cudaSuccess)
         return e;
+    // ctas_per_sm > 0: the smallest shared-memory carve-out that holds that many
+    // CTAs, so the rest of the SM's unified L1 / shared memory is L1 (the
+    // explorers read trees, radii and unstaged scene data through it); measured
+    // faster than the largest carve-out's one more resident CTA per SM.  The
+    // attribute belongs to the kernel, so every launch sets it (-1: no preference).
+    int carve = -1;
+    if (L.persistent && L.ctas_per_sm > 0) {
+        int dev = 0, sm_smem = 0, reserved = 0;
+        cudaFuncAttributes fa;
+        cudaGetDevice(&dev);
+        if ((e = cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess ||
+            (e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess ||
+            (e = cudaFuncGetAttributes(&fa, kern)) != cudaSuccess)
+            return e;
+        const size_t need = (size_t)L.ctas_per_sm * (dyn + fa.sharedSizeBytes + (size_t)reserved);
+        carve = sm_smem > 0 ? (int)std::min<size_t>(100, (100 * need + sm_smem - 1) / (size_t)sm_smem) : -1;
+    }
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, carve)) != cudaSuccess)
+        return e;
     if (L.persistent) {
         int per_sm = 0;
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, dyn)) != cudaSuccess) return e;
         per_sm = std::max(per_sm, 1);
+        if (L.ctas_per_sm > 0) per_sm = std::min(per_sm, L.ctas_per_sm);
         long long grid = (long long)per_sm * device_sm_count();
         if (L.resident > 0) grid = std::min<long long>(grid, L.resident);
         const long long work = warps ? (long long)L.B * ((L.E + kWarpsPerCta - 1) / kWarpsPerCta) : (long long)L.B * L.E;

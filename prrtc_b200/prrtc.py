@@ -23,7 +23,9 @@ Differences from the reference, all deliberate:
     ``num_new_samples`` explorers per problem, as the reference), and
     ``point_cloud`` / ``r_env`` (an environment point cloud checked inside the
     kernel, shared by the batch; a collision_context's ``point_cloud`` entry
-    does the same).
+    does the same), and ``ctas_per_sm`` (persistent launch: at most that many
+    CTAs per SM with a shared-memory carve-out that just holds them, leaving
+    the rest of the SM's memory to L1).
 """
 from __future__ import annotations
 
@@ -117,8 +119,9 @@ def _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio,
 
 
 def _tuning(edge_resolution=0.0, threads_per_explorer=0, waypoint_chunk=0, resident_ctas=0,
-            tail_explorers=True) -> _lib.Tuning:
+            tail_explorers=True, ctas_per_sm=0) -> _lib.Tuning:
     t = _lib.Tuning()
+    t.ctas_per_sm = int(ctas_per_sm or 0)
     t.tail_explorers = 0 if tail_explorers else -1
     t.edge_resolution = float(edge_resolution or 0.0)
     t.threads_per_explorer = int(threads_per_explorer or 0)
@@ -497,6 +500,7 @@ def prrtc_plan_batch_async(
     point_cloud=None,
     r_env: float = 0.02,
     tail_explorers: bool = True,
+    ctas_per_sm: int = 0,
     device=None,
 ) -> "PendingBatch":
     """Plan B independent problems (prrtc.py:882-1434), without waiting: the
@@ -633,7 +637,7 @@ def prrtc_plan_batch_async(
         bi.problem_capacity = stage.get(k_caps).data_ptr()
     attrs = _attrs(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio, dynamic_domain, dd_alpha,
                    dd_radius, dd_min_radius, dim, max_nodes, granularity, collision_mode, collision_margin)
-    tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk, resident_ctas, tail_explorers)
+    tun = _tuning(edge_resolution, threads_per_explorer, waypoint_chunk, resident_ctas, tail_explorers, ctas_per_sm)
     from .pointcloud import PointCloud, cloud_from_context
 
     # one environment point cloud for the whole batch: a PointCloud, or the

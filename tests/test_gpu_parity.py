@@ -275,11 +275,13 @@ def test_plan_solves_and_revalidates(cuda, orc, kind, seed, checker):
     _check_tree_sound(sc, r.tree_b_configs.cpu().numpy(), r.tree_b_parents.cpu().numpy(), r.tree_b_size, pr.dim)
 
 
-@pytest.mark.parametrize("launch,threads", [("persistent", 128), ("persistent", 32), ("per_problem", 128),
-                                            ("per_problem", 32)])
-def test_batch_uneven_solves(cuda, orc, launch, threads):
+@pytest.mark.parametrize("launch,threads,ctas", [("persistent", 128, 0), ("persistent", 32, 0),
+                                                 ("persistent", 128, 2), ("persistent", 32, 2),
+                                                 ("per_problem", 128, 0), ("per_problem", 32, 0)])
+def test_batch_uneven_solves(cuda, orc, launch, threads, ctas):
     """threads=32 with the persistent launch runs one explorer per warp, four
-    explorers of a problem per CTA."""
+    explorers of a problem per CTA; ctas=2 caps the persistent grid at two CTAs
+    per SM with the smaller shared-memory carve-out."""
     from prrtc_b200 import prrtc_plan_batch
 
     probs = [make_problem("uneven", 100 + i) for i in range(12)]
@@ -292,7 +294,7 @@ def test_batch_uneven_solves(cuda, orc, launch, threads):
                            max_nodes=16384, min_vals=probs[0].lower, max_vals=probs[0].upper,
                            collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
                            goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01, launch=launch,
-                           threads_per_explorer=threads)
+                           threads_per_explorer=threads, ctas_per_sm=ctas)
     assert len(res) == len(probs)
     assert sum(r.solved for r in res) >= len(probs) - 1
     for i, (p, r) in enumerate(zip(probs, res)):
