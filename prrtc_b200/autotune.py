@@ -5,7 +5,7 @@ candidate (explorers per problem = samples per iteration, threads per explorer
 -- 32 meaning one explorer per warp, four per CTA --, waypoints per
 shared-memory chunk, CTAs per SM) by solved plans per second: the median of three launches
 per candidate, then a second round between the three best (six more launches
-each, taken in turn) decides.  Results
+each, taken in turn) decides; L2 is flushed before every timed launch.  Results
 are cached per (device, bucket, problem count, shape) in
 ``~/.cache/prrtc_b200/autotune.json``.
 """
@@ -42,7 +42,9 @@ def _load() -> dict:
         return {}
 
 
-def _rate(pl) -> float:
+def _rate(pl, flush=None) -> float:
+    if flush is not None:  # evict L2 outside the timed events, as the bench does between steps
+        flush.fill_(1.0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     pl.launch()
@@ -64,7 +66,7 @@ def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = 
     launches wins."""
     from .batch import BatchPlanner, PlanSettings
 
-    key = "v7|" + _key(dev, N, problems, settings)
+    key = "v8|" + _key(dev, N, problems, settings)
     cache = _load() if use_cache else {}
     if key in cache:
         return dict(cache[key])
@@ -78,12 +80,16 @@ def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = 
     def med(r):
         return sorted(r)[len(r) // 2]
 
+    # a 256 MB write between timed launches leaves L2 (126 MB on B200) cold,
+    # the condition the bench times: with a warm L2 the L1 share of a
+    # candidate (ctas_per_sm) matters less than it does then
+    flush = torch.empty(64 * 2**20, dtype=torch.float32, device=dev)
     rates = {}
     for c in candidates:
         pl = planner(c)
         pl.launch()  # warm
         torch.cuda.synchronize(dev)
-        rates[c] = [_rate(pl) for _ in range(3)]
+        rates[c] = [_rate(pl, flush) for _ in range(3)]
         del pl
     top = sorted(candidates, key=lambda c: -med(rates[c]))[:max(1, finalists)]
     if len(top) > 1:
@@ -93,7 +99,7 @@ def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = 
         torch.cuda.synchronize(dev)
         for _ in range(final_reps):
             for c in top:
-                rates[c].append(_rate(pls[c]))
+                rates[c].append(_rate(pls[c], flush))
         del pls
     best = max(top, key=lambda c: med(rates[c]))
     best = {"num_new_samples": best[0], "threads_per_explorer": best[1], "waypoint_chunk": best[2],
