@@ -18,7 +18,7 @@ from pathlib import Path
 import torch
 
 SAMPLES = (1, 2, 4, 8, 16)
-THREADS = (64, 128)  # 32 (one explorer per warp) stays available but lost on every bucket measured
+THREADS = (64, 128, 256)  # 32 (one explorer per warp) stays available but lost on every bucket measured
 CHUNKS = (8, 16, 32)
 CTAS_PER_SM = (0, 2)  # 0: as many as fit; 2: two, with the rest of shared memory given to L1
 CANDIDATES = tuple((e, t, c, r) for r in CTAS_PER_SM for t in THREADS for c in CHUNKS for e in SAMPLES)
@@ -66,7 +66,7 @@ def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = 
     launches wins."""
     from .batch import BatchPlanner, PlanSettings
 
-    key = "v8|" + _key(dev, N, problems, settings)
+    key = "v9|" + _key(dev, N, problems, settings)
     cache = _load() if use_cache else {}
     if key in cache:
         return dict(cache[key])
