@@ -158,8 +158,10 @@ PyObject* scan(PyObject*, PyObject* args) {
 
 // fill(contexts, specs, layout, out): layout per spec is (shared, max_rows,
 // table_offset, counts_offset); a shared spec copies context 0's table, the
-// others write a zero-padded [B, max_rows, feat] table and int32[B] counts
-// (counts_offset < 0: no counts).  Offsets are bytes into the writable `out`.
+// others write the rows of a [B, max_rows, feat] table and int32[B] counts
+// (counts_offset < 0: no counts).  Rows past a problem's count are left as
+// they were: the planner reads only counted rows.  Offsets are bytes into
+// the writable `out`.
 PyObject* fill(PyObject*, PyObject* args) {
     PyObject *contexts, *specs, *layout, *outobj;
     if (!PyArg_ParseTuple(args, "OOOO", &contexts, &specs, &layout, &outobj)) return nullptr;
@@ -203,7 +205,6 @@ PyObject* fill(PyObject*, PyObject* args) {
             ok = false;
             break;
         }
-        std::memset(base + toff, 0, (size_t)tb);
         for (Py_ssize_t i = 0; i < B; ++i) {
             const Table& t = tabs.t[(size_t)i];
             if (t.rows > mx) {

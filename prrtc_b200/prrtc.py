@@ -198,17 +198,19 @@ class _Results:
         rows = host.tolist()
         kts = host[:, 9].copy().view(np.float32).tolist()
         costs = host[:, 11].copy().view(np.float32).tolist()
+        inf = float("inf")
+        make = tuple.__new__  # positional construction: the loop runs once per problem
+        from_numpy = torch.from_numpy
         for i in range(self.B):
             row = rows[i]
             solved = row[8] == 1
             size_a, size_b = row[0], row[1]
             length = row[10]
-            kt = kts[i]
-            cost = costs[i] if solved else float("inf")
+            cost = costs[i] if solved else inf
             path = None
             if solved:
                 if length > 0:
-                    path = torch.from_numpy(hpaths[i, :length]) if hpaths is not None else self.paths[i, :length]
+                    path = from_numpy(hpaths[i, :length]) if hpaths is not None else self.paths[i, :length]
                 else:  # longer than the device path buffer: walk on the host
                     path = self._host_trace(i)
                     cost = float(torch.linalg.norm(torch.diff(path, dim=0), dim=1).sum())
@@ -223,11 +225,8 @@ class _Results:
                 tbc = (self.tb[i] if batched else self.tb)[:, :nb]
                 tap = (self.pa[i] if batched else self.pa)[:na]
                 tbp = (self.pb[i] if batched else self.pb)[:nb]
-            out.append(PRRTCResult(
-                solved=solved, path=path, tree_a_size=size_a, tree_b_size=size_b, iterations=row[4],
-                cost=cost, kernel_time_ms=kt, tree_a_configs=tac, tree_b_configs=tbc, tree_a_parents=tap,
-                tree_b_parents=tbp,
-            ))
+            # field order of PRRTCResult
+            out.append(make(PRRTCResult, (solved, path, size_a, size_b, row[4], cost, kts[i], tac, tbc, tap, tbp)))
         return out
 
     def _host_trace(self, i: int) -> torch.Tensor:
@@ -412,7 +411,8 @@ def _native_pack(contexts: Sequence[Optional[dict]], stage: Stager):
     """The world / self tables of every context packed by the native host
     packer straight into the call's pinned staging buffer: padded
     [B, max_n, feat] tables + int32 counts, or one copy of a table every
-    context shares (same layout as _pack_worlds / _shared_table).  Returns
+    context shares (same layout as _pack_worlds / _shared_table; rows past a
+    problem's count are left unwritten, the planner never reads them).  Returns
     ({key: (table key, counts key or None, width)}, {key: counts}), or None
     when some table is not a C-contiguous float32 / int32 numpy array (the
     Python packer then handles the call)."""
