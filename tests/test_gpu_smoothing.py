@@ -1,5 +1,6 @@
 """Adjoint smoothing kernel: cost against the float64 oracle, gradient against
-central finite differences (h = 1e-3) of the oracle cost, the autograd wrapper,
+central finite differences (h = 1e-3) of the oracle cost and against
+torch.autograd of a float64 restatement of the cost, the autograd wrapper,
 and the smoothing pass (accepted paths re-validate, rejected ones revert)."""
 from __future__ import annotations
 
@@ -47,6 +48,26 @@ def test_adjoint_matches_finite_differences(cuda, orc, kind, seed):
     g_fd = _fd_grad(sc, w.astype(np.float64))
     g = grad[0].cpu().numpy().astype(np.float64)
     rel = np.linalg.norm(g - g_fd) / np.linalg.norm(g_fd)
+    assert rel < 1e-3, rel
+
+
+@pytest.mark.parametrize("kind,seed", [("tabletop", 3), ("spheres16", 1), ("uneven", 7)])
+def test_adjoint_matches_autodiff_reference(cuda, orc, kind, seed):
+    """The adjoint kernel against torch.autograd of a float64 restatement of
+    the same cost (oracle/smooth_autodiff.py), the stand-in for jax.grad of a
+    pure-JAX FK + SDF reference (jax is not installed: the jax check is not
+    run).  Tolerance as for the central differences: 1e-3 relative."""
+    from oracle.smooth_autodiff import smooth_grad
+    from prrtc_b200.smoothing import SmoothContext, resample_path
+
+    pr, sc, path = _solved_path(orc, kind, seed)
+    w = resample_path(path, 16)
+    sctx = SmoothContext(pr.context, pr.dim, MARGIN, BETA, WLEN, cuda)
+    cost, grad = sctx.cost_grad(torch.from_numpy(w)[None].to(cuda))
+    c_ad, g_ad = smooth_grad(pr.context, w.astype(np.float64), MARGIN, BETA, WLEN)
+    assert abs(cost.item() - c_ad) <= 1e-4 * max(1.0, abs(c_ad))
+    g = grad[0].cpu().numpy().astype(np.float64)
+    rel = np.linalg.norm(g - g_ad) / np.linalg.norm(g_ad)
     assert rel < 1e-3, rel
 
 

@@ -321,3 +321,26 @@ def test_point_cloud_stage_brute_force(orc, arm):
         if abs(d.min()) > 1e-6:
             assert v[i] == int(d.min() <= 0)
     assert 0 < v.sum() < q.shape[0]
+
+
+@pytest.mark.parametrize("kind,seed", [("tabletop", 3), ("spheres16", 1), ("uneven", 7)])
+def test_autodiff_reference_matches_oracle_cost_and_differences(orc, kind, seed):
+    """The autograd restatement of the smoothing cost (the stand-in for a
+    jax.grad reference) agrees with the C oracle's cost, and its gradient with
+    central differences of that cost."""
+    from oracle.smooth_autodiff import smooth_grad
+
+    pr = make_problem(kind, seed)
+    sc = orc.Scene(pr.context, pr.dim)
+    rng = np.random.default_rng(seed)
+    w = np.linspace(pr.start, pr.goals[0], 6).astype(np.float64) + rng.normal(0, 0.05, (6, pr.dim))
+    c, g = smooth_grad(pr.context, w, 0.02, 50.0, 1.0)
+    c64 = sc.smooth_cost(w, 0.02, 50.0, 1.0)
+    assert abs(c - c64) <= 1e-9 * max(1.0, abs(c64))
+    h = 1e-5
+    for i, d in [(1, 0), (2, 3), (4, 6), (3, 1)]:
+        wp, wm = w.copy(), w.copy()
+        wp[i, d] += h
+        wm[i, d] -= h
+        fd = (sc.smooth_cost(wp, 0.02, 50.0, 1.0) - sc.smooth_cost(wm, 0.02, 50.0, 1.0)) / (2 * h)
+        assert abs(g[i, d] - fd) <= 1e-5 * max(1.0, abs(fd)), (i, d, g[i, d], fd)
