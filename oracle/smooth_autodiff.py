@@ -176,4 +176,4 @@ def smooth_grad(ctx: dict, waypoints: np.ndarray, margin: float = 0.02, beta: fl
     x = torch.tensor(np.asarray(waypoints, dtype=np.float64), requires_grad=True)
     cost = smooth_cost(ctx, x, margin, beta, w_len)
     (g,) = torch.autograd.grad(cost, x)
-    return float(cost), g.numpy()
+    return float(cost.detach()), g.numpy()
