@@ -395,6 +395,27 @@ def run_ours(a):
     }
     line["gpu_launches"] = 5 * len(planners) * a.steps  # per planner: pack, init, explore, finalize, paths
 
+    # e2e on every rank (each its own problems), whole job = all ranks' plans
+    # over the slowest rank's seconds
+    if not a.no_extras:
+        if ws > 1:
+            dist.barrier()
+        e_solved, e_s, e_h2d, e_d2h, e_steps = measure_e2e(torch, dev, planners, settings, tuned, cap_of)
+        if ws > 1:
+            v = torch.tensor([e_s, float(e_solved), float(e_h2d), float(e_d2h)], dtype=torch.float64, device=dev)
+            vmax = v[:1].clone()
+            dist.all_reduce(vmax, op=dist.ReduceOp.MAX)
+            vsum = v[1:].clone()
+            dist.all_reduce(vsum, op=dist.ReduceOp.SUM)
+            e_s, e_solved, e_h2d, e_d2h = float(vmax.item()), *(float(x) for x in vsum.tolist())
+        line["e2e"] = {"value": e_solved / e_s, "unit": "plans/s", "h2d_bytes_per_step": int(e_h2d),
+                       "d2h_bytes_per_step": int(e_d2h), "steps": e_steps,
+                       "api": "prrtc_b200.prrtc_plan_batch_async + .results() (per-problem collision_context "
+                              "dicts, host numpy inputs, one call per step for all of a rank's problems, up to "
+                              "three steps in flight on three streams: later steps are packed and copied while "
+                              "the oldest plans; paths copied to the host; whole job: every rank, slowest "
+                              "rank's time)"}
+
     if rank == 0 and not a.no_extras:
         line.update(extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of))
     if rank == 0:
@@ -451,8 +472,61 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     out["planner_edges_per_s"] = edges / (ms * 1e-3)
     out["planner_nn_gbs"] = nn_nodes * 7 * 4 / (ms * 1e-3) / 1e9
 
-    # --- e2e through the public API with host inputs (numpy), results + paths back to host
+    # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
+    from prrtc_b200.batch import bucket_problems
+
+    def plain(ps_all):
+        solved = 0
+        for N, ps in bucket_problems(ps_all).items():
+            G = max(p.goals.shape[0] for p in ps)
+            goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
+            for i, p in enumerate(ps):
+                goals[i, : p.goals.shape[0]] = p.goals
+            res = prrtc_plan_batch(np.stack([p.start for p in ps]), goals, max_iterations=settings.max_iterations,
+                                   num_new_samples=128, max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper,
+                                   collision_context=[p.context for p in ps],
+                                   collision_checker=settings.collision_checker,
+                                   goal_counts=[p.goals.shape[0] for p in ps],
+                                   edge_resolution=settings.edge_resolution, launch="per_problem",
+                                   return_trees=False)
+            solved += sum(r.solved for r in res)
+        return solved
+
+    plain(problems)  # warm: first-call stream and workspace set-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    solved_plain = plain(problems)
+    torch.cuda.synchronize()
+    dtp = time.perf_counter() - t0
+    out["plain_per_problem"] = {"plans_per_s": solved_plain / dtp, "success_rate": solved_plain / len(problems),
+                                "note": "one plain planner launch per problem over 8 streams, 128 explorers each, "
+                                        "host-timed incl. per-problem set-up (the reference's batch form); "
+                                        "second of two passes"}
+    out["batched_vs_plain"] = line["value"] / max(out["plain_per_problem"]["plans_per_s"], 1e-9)
+
+    out.update(measure_cc(torch, dev, fp32))
+    out.update(measure_nn(torch, dev, peaks))
+    out.update(measure_smooth(torch, dev))
+
+    # --- CPU baseline (the reference's host loop restated), 1 core, bounded sample
+    from oracle import oracle as O
+
+    O.build()
+    cb = cpu_baseline(problems, a.cpu_seconds, 1)
+    out["cpu_baseline"] = {"value": cb["plans_per_s"], "unit": "plans/s", "cores": 1, "kind": "port",
+                           "sample": f"first {cb['done']} problems of the workload in {cb['seconds']:.1f} s, "
+                                     f"host-driven RRT-Connect restated in C (prrtc_robogpu.py:103-298), "
+                                     f"{cpu_model()}"}
+    return out
+
+
+def measure_e2e(torch, dev, planners, settings, tuned, cap_of):
+    """End to end through the public API on this rank: host numpy inputs copied
+    in and results plus paths copied back inside the timed region.  Returns
+    (plans solved, seconds, host->device bytes per step, device->host bytes per
+    step, steps)."""
     from prrtc_b200 import device as _device
+    from prrtc_b200.prrtc import prrtc_plan_batch_async
 
     # One public call per step for all problems, up to three in flight on
     # three streams: the host packs and copies the next steps while the device
@@ -510,59 +584,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
         d2h += d_
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    out["e2e"] = {"value": solved / dt, "unit": "plans/s", "h2d_bytes_per_step": _device.H2D_BYTES[0] // k_e2e,
-                  "d2h_bytes_per_step": d2h // k_e2e, "steps": k_e2e,
-                  "api": "prrtc_b200.prrtc_plan_batch_async + .results() (per-problem collision_context dicts, "
-                         "host numpy inputs, one call per step for all problems, up to three steps in flight "
-                         "on three streams: later steps are packed and copied while the oldest plans; paths "
-                         "copied to the host)"}
-
-    # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
-    from prrtc_b200.batch import bucket_problems
-
-    def plain(ps_all):
-        solved = 0
-        for N, ps in bucket_problems(ps_all).items():
-            G = max(p.goals.shape[0] for p in ps)
-            goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
-            for i, p in enumerate(ps):
-                goals[i, : p.goals.shape[0]] = p.goals
-            res = prrtc_plan_batch(np.stack([p.start for p in ps]), goals, max_iterations=settings.max_iterations,
-                                   num_new_samples=128, max_nodes=N, min_vals=ps[0].lower, max_vals=ps[0].upper,
-                                   collision_context=[p.context for p in ps],
-                                   collision_checker=settings.collision_checker,
-                                   goal_counts=[p.goals.shape[0] for p in ps],
-                                   edge_resolution=settings.edge_resolution, launch="per_problem",
-                                   return_trees=False)
-            solved += sum(r.solved for r in res)
-        return solved
-
-    plain(problems)  # warm: first-call stream and workspace set-up
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    solved_plain = plain(problems)
-    torch.cuda.synchronize()
-    dtp = time.perf_counter() - t0
-    out["plain_per_problem"] = {"plans_per_s": solved_plain / dtp, "success_rate": solved_plain / len(problems),
-                                "note": "one plain planner launch per problem over 8 streams, 128 explorers each, "
-                                        "host-timed incl. per-problem set-up (the reference's batch form); "
-                                        "second of two passes"}
-    out["batched_vs_plain"] = line["value"] / max(out["plain_per_problem"]["plans_per_s"], 1e-9)
-
-    out.update(measure_cc(torch, dev, fp32))
-    out.update(measure_nn(torch, dev, peaks))
-    out.update(measure_smooth(torch, dev))
-
-    # --- CPU baseline (the reference's host loop restated), 1 core, bounded sample
-    from oracle import oracle as O
-
-    O.build()
-    cb = cpu_baseline(problems, a.cpu_seconds, 1)
-    out["cpu_baseline"] = {"value": cb["plans_per_s"], "unit": "plans/s", "cores": 1, "kind": "port",
-                           "sample": f"first {cb['done']} problems of the workload in {cb['seconds']:.1f} s, "
-                                     f"host-driven RRT-Connect restated in C (prrtc_robogpu.py:103-298), "
-                                     f"{cpu_model()}"}
-    return out
+    return solved, dt, _device.H2D_BYTES[0] // k_e2e, d2h // k_e2e, k_e2e
 
 
 def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
