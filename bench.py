@@ -464,7 +464,11 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
         del ip
     achieved = flops / (ms * 1e-3) / 1e12
     out["roofline"] = {"kernel": "explore_kernel (persistent planner)", "bound": "fp32", "achieved": achieved,
-                       "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32, "traffic": None,
+                       "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
+                       # DRAM bytes of one planner launch of this workload from one ncu capture
+                       # (dram__bytes.sum.per_second x gpu__time_duration, profiles/explore_kernel_uneven512_eager.md):
+                       # the trees, radii and scenes live in L1/L2, so the planner hardly touches HBM
+                       "traffic": 7.4e6, "traffic_unit": "bytes per launch (ncu)",
                        "peak_source": "measured in bench.py by the FFMA probe (no FP32 entry in MEASURED_PEAKS.json)",
                        "note": "collision FLOPs actually executed (device counters) / planner time; the planner is "
                                "latency-bound by its dependent sample->NN->extend->check iterations"}
