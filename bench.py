@@ -623,7 +623,10 @@ def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
     return {"cc_kernel": {"workload": f"tabletop scene (32 spheres, 8 capsules, 20 boxes, 1 halfspace), {n} configs, "
                                       "flat checker, full sweep", "checks_per_s": n / (best * 1e-3),
                           "flops_per_check": f_cfg, "achieved_tflops": ach,
-                          "frac_of_fp32_peak": (ach / fp32) if fp32 else None}}
+                          "frac_of_fp32_peak": (ach / fp32) if fp32 else None,
+                          # one ncu capture (profiles/check_kernel_tabletop_fullsweep.md): the
+                          # configurations, read once; the scene lives in shared memory
+                          "traffic_bytes_ncu": 29.45e6}}
 
 
 def measure_smooth(torch, dev, paths: int = 512, waypoints: int = 64, launches: int = 20, reps: int = 3):
@@ -714,6 +717,8 @@ def measure_nn(torch, dev, peaks, reps: int = 3, launches: int = 20):
     return {"nn_kernel": {"workload": "1 query x 33554432 nodes x 7 dims (940 MB tree, HBM-streamed)",
                           "ms": ms_h, "achieved_gbs": gbs_h, "hbm_peak_gbs": hbm,
                           "frac": gbs_h / hbm if hbm else None,
+                          # one ncu capture (profiles/nn_kernel_1q_32M_hbm.md): 6.34 TB/s x 148.9 us
+                          "traffic_bytes_ncu": 944e6,
                           "note": "algorithmic bytes = nodes x dim x 4 per query; per-launch time of 20 "
                                   "back-to-back launches (init of the 64-bit argmin keys, scan, decode)"},
             "nn_kernel_l2": {"workload": "64 queries x 4194304 nodes x 7 dims (117 MB tree, L2-resident)",
