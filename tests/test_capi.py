@@ -197,3 +197,45 @@ def test_native_host_packer_declines_other_types():
     layout, total = _native_layout(info, _PACK_SPECS, 2)
     with pytest.raises(ValueError):
         hp.fill([good, good], _PACK_SPECS, layout, np.zeros(max(total - 1, 0), np.uint8))
+
+
+def test_autotuner_second_round_decides(monkeypatch):
+    """Host logic of the autotuner: every candidate gets three timed launches,
+    the three best by median six more each, and the best median over all of a
+    finalist's launches wins -- so a candidate that was lucky in the first
+    round loses to a steadily faster one.  Fake planners, no GPU."""
+    import torch
+
+    from prrtc_b200 import autotune, batch
+
+    class FakePlanner:
+        def __init__(self, problems, N, s, dev):
+            self.key = (s.num_new_samples, s.threads_per_explorer, s.waypoint_chunk, s.ctas_per_sm)
+
+        def launch(self):
+            pass
+
+    cands = ((1, 128, 32, 0), (2, 128, 32, 0), (4, 128, 32, 0), (2, 256, 32, 2))
+    # first three timed launches, then the second-round launches
+    script = {
+        (1, 128, 32, 0): [100, 100, 100] + [100] * 6,
+        (2, 128, 32, 0): [300, 300, 300] + [110] * 6,    # lucky first round, slower after
+        (4, 128, 32, 0): [90, 90, 90] + [90] * 6,
+        (2, 256, 32, 2): [150, 150, 150] + [200] * 6,    # steadily the fastest
+    }
+    calls = []
+
+    def fake_rate(pl, flush=None):  # the script runs on per candidate, across planner objects
+        r = script[pl.key][calls.count(pl.key)]
+        calls.append(pl.key)
+        return float(r)
+
+    monkeypatch.setattr(batch, "BatchPlanner", FakePlanner)
+    monkeypatch.setattr(autotune, "_rate", fake_rate)
+    monkeypatch.setattr(autotune, "_key", lambda *a: "fake")
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    best = autotune.choose([object()], 4096, batch.PlanSettings(), torch.device("cpu"), candidates=cands,
+                           use_cache=False)
+    assert best == {"num_new_samples": 2, "threads_per_explorer": 256, "waypoint_chunk": 32, "ctas_per_sm": 2}
+    assert calls.count((4, 128, 32, 0)) == 3          # not a finalist
+    assert calls.count((2, 256, 32, 2)) == 9          # finalist: 3 + 6
