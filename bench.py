@@ -479,8 +479,11 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
     from prrtc_b200.batch import bucket_problems
 
+    plain_ms = []
+
     def plain(ps_all):
         solved = 0
+        plain_ms.clear()
         for N, ps in bucket_problems(ps_all).items():
             G = max(p.goals.shape[0] for p in ps)
             goals = np.zeros((len(ps), G, ps[0].dim), np.float32)
@@ -494,6 +497,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
                                    edge_resolution=settings.edge_resolution, launch="per_problem",
                                    return_trees=False)
             solved += sum(r.solved for r in res)
+            plain_ms.extend(r.kernel_time_ms for r in res if r.solved and r.kernel_time_ms is not None)
         return solved
 
     plain(problems)  # warm: first-call stream and workspace set-up
@@ -503,6 +507,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     torch.cuda.synchronize()
     dtp = time.perf_counter() - t0
     out["plain_per_problem"] = {"plans_per_s": solved_plain / dtp, "success_rate": solved_plain / len(problems),
+                                "p50_solve_ms": float(np.median(plain_ms)) if plain_ms else None,
                                 "note": "one plain planner launch per problem over 8 streams, 128 explorers each, "
                                         "host-timed incl. per-problem set-up (the reference's batch form); "
                                         "second of two passes"}
