@@ -3,19 +3,25 @@
 
 Workload (one "step"): 512 planning problems for the synthetic 7-DOF arm, each
 with its own world (4-128 spheres, 0-32 boxes) and 1-8 goals, tree capacity
-bucketed to 4096 / 16384 / 65536 nodes by world size; every problem is solved
-once per step by the persistent batched planner (one captured CUDA graph per
-bucket).  Problems are seeded synthetic stand-ins for the reference's MBM sets.
+4096 / 16384 / 65536 nodes by world size; every problem is solved once per
+step by the persistent batched planner, all problems in one launch with
+per-problem capacities (one captured CUDA graph; --launch buckets: one graph
+per capacity on concurrent streams), settings chosen by the autotuner
+(--tuning fixes them).  Problems are seeded synthetic stand-ins for the
+reference's MBM sets.
 
-  value  plans/s with inputs resident in HBM (graph replays, CUDA events)
-  e2e    plans/s through the public API prrtc_plan_batch with host inputs:
-         host->device copies and the device->host read of results and paths
-         inside the timed region
+  value  plans/s with inputs resident in HBM (graph replays, CUDA events,
+         L2 flushed between steps)
+  e2e    plans/s through the public API prrtc_plan_batch_async + results()
+         with host inputs: host->device copies and the device->host read of
+         results and paths inside the timed region, up to three calls in
+         flight; at N GPUs every rank runs it and the slowest rank's time counts
 
-Also reported: the plain per-problem-launch form on the same GPU (the
-reference's batch structure), p50 device solve ms, collision checks/s of the
-planner and of the standalone FK+collision kernel, nearest-neighbour GB/s,
-each kernel's roofline fraction, and the CPU baseline (the reference's
+Also reported (rank 0): the plain per-problem-launch form on the same GPU
+(the reference's batch structure) with its p50 device solve ms, collision
+checks/s of the planner and of the standalone FK+collision kernel,
+nearest-neighbour GB/s, the smoothing adjoint's waypoint gradients/s, each
+kernel's roofline fraction, and the CPU baseline (the reference's
 host-driven RRT-Connect loop restated in C, timed on this host).
 
 Multi-GPU (torchrun): weak scaling -- every rank solves its own 512 problems
