@@ -277,7 +277,9 @@ def test_plan_solves_and_revalidates(cuda, orc, kind, seed, checker):
 
 @pytest.mark.parametrize("launch,threads,ctas", [("persistent", 128, 0), ("persistent", 32, 0),
                                                  ("persistent", 128, 2), ("persistent", 32, 2),
-                                                 ("per_problem", 128, 0), ("per_problem", 32, 0)])
+                                                 ("persistent", 256, 2), ("persistent", 64, 0),
+                                                 ("per_problem", 128, 0), ("per_problem", 32, 0),
+                                                 ("per_problem", 256, 0)])
 def test_batch_uneven_solves(cuda, orc, launch, threads, ctas):
     """threads=32 with the persistent launch runs one explorer per warp, four
     explorers of a problem per CTA; ctas=2 caps the persistent grid at two CTAs
@@ -311,7 +313,8 @@ def test_batch_uneven_solves(cuda, orc, launch, threads, ctas):
             _check_tree_sound(sc, r.tree_b_configs.cpu().numpy(), r.tree_b_parents.cpu().numpy(), r.tree_b_size, dim)
 
 
-def test_batch_dual_arm_large_world(cuda, orc):
+@pytest.mark.parametrize("threads,ctas", [(128, 0), (256, 2)])
+def test_batch_dual_arm_large_world(cuda, orc, threads, ctas):
     """Dual-arm workload: 14 joints (18 with 4 mimic gripper joints), 120
     spheres, 256 spheres + 64 boxes + floor, 131072-node trees, 1-4 goals."""
     from prrtc_b200 import prrtc_plan_batch
@@ -326,7 +329,8 @@ def test_batch_dual_arm_large_world(cuda, orc):
     res = prrtc_plan_batch(np.stack([p.start for p in probs]), goals, max_iterations=10000, num_new_samples=64,
                            max_nodes=131072, min_vals=probs[0].lower, max_vals=probs[0].upper,
                            collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
-                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01)
+                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01,
+                           threads_per_explorer=threads, ctas_per_sm=ctas)
     assert sum(r.solved for r in res) >= len(probs) - 1
     for p, r in zip(probs, res):
         if not r.solved:
