@@ -239,3 +239,54 @@ def test_autotuner_second_round_decides(monkeypatch):
     assert best == {"num_new_samples": 2, "threads_per_explorer": 256, "waypoint_chunk": 32, "ctas_per_sm": 2}
     assert calls.count((4, 128, 32, 0)) == 3          # not a finalist
     assert calls.count((2, 256, 32, 2)) == 9          # finalist: 3 + 6
+
+
+def test_native_host_packer_random_contexts():
+    """Seeded random batches (ragged tables, absent keys, None contexts, shared
+    and equal-content tables): the native packer's counted rows, counts and
+    shared tables equal the Python packer's."""
+    from prrtc_b200 import _lib
+    from prrtc_b200.prrtc import _PACK_SPECS, _pack_worlds, _shared_table
+
+    hp = _lib.hostpack()
+    feats = {k: f for k, f, _ in _PACK_SPECS}
+    for seed in range(25):
+        rng = np.random.default_rng(1000 + seed)
+        B = int(rng.integers(1, 40))
+        shared = {k: rng.normal(size=(int(rng.integers(0, 5)), f)).astype(np.int32 if k == "self_pairs" else np.float32)
+                  for k, f in feats.items()}
+        ctxs = []
+        for i in range(B):
+            if rng.random() < 0.05:
+                ctxs.append(None)
+                continue
+            c = {}
+            for k, f in feats.items():
+                u = rng.random()
+                dt = np.int32 if k == "self_pairs" else np.float32
+                if u < 0.15:
+                    continue                                     # absent
+                if u < 0.45:
+                    c[k] = shared[k] if rng.random() < 0.5 else shared[k].copy()   # same object / same content
+                else:
+                    c[k] = (rng.normal(size=(int(rng.integers(0, 9)), f)) * 10).astype(dt)
+            ctxs.append(c)
+        info = hp.scan(ctxs, _PACK_SPECS)
+        layout, total = _native_layout(info, _PACK_SPECS, B)
+        buf = np.full(total + 32, 0x5A, np.uint8)
+        hp.fill(ctxs, _PACK_SPECS, layout, buf)
+        sh = {k: _shared_table(ctxs, k) for k in feats}
+        packed, counts = _pack_worlds(ctxs, B, skip={k for k in sh if sh[k] is not None})
+        for (key, feat, kind), (is_sh, width, cbytes), (_, _, off, coff) in zip(_PACK_SPECS, info, layout):
+            dt = np.int32 if kind == "i" else np.float32
+            assert is_sh == (sh[key] is not None), (seed, key)
+            if is_sh:
+                assert np.array_equal(buf[off:off + sh[key].nbytes].view(dt).reshape(sh[key].shape), sh[key])
+            else:
+                ref = packed[key]
+                got = buf[off:off + ref.nbytes].view(dt).reshape(ref.shape)
+                n = counts[key]
+                assert np.array_equal(buf[coff:coff + 4 * B].view(np.int32), n), (seed, key)
+                for i in range(B):
+                    assert np.array_equal(got[i, :n[i]], ref[i, :n[i]]), (seed, key, i)
+        assert (buf[total:] == 0x5A).all()
