@@ -503,3 +503,46 @@ def test_batch_per_problem_capacity(cuda, orc):
             assert ok, md
     assert sum(r.solved for r in res[:5]) >= 4
     assert not res[5].solved and max(res[5].tree_a_size, res[5].tree_b_size) >= 2
+
+
+@pytest.mark.parametrize("launch", ["persistent", "per_problem"])
+def test_batch_mixed_full_and_trimmed_contexts(cuda, orc, launch):
+    """The reference's batch scenario (test_prrtc.py:408-491): four problems
+    whose contexts alternate between the full scene and one with the last
+    world sphere and the last self pair removed, one goal each, step 0.6, 16
+    samples, dynamic domain off.  Every solved path, and a sample of each
+    solved problem's start tree, re-validates against that problem's own
+    context (full or trimmed)."""
+    from prrtc_b200 import prrtc_plan_batch
+
+    base = make_problem("spheres16", 11)
+    full = base.context
+    trimmed = dict(full)
+    trimmed["world_spheres"] = np.ascontiguousarray(full["world_spheres"][:-1])
+    trimmed["self_pairs"] = np.ascontiguousarray(full["self_pairs"][:-1])
+    ctxs = [full if i % 2 == 0 else trimmed for i in range(4)]
+    rng = np.random.default_rng(11)
+    starts, goals = [], []
+    for i in range(4):
+        sc = orc.Scene(ctxs[i], base.dim)
+        pair = []
+        while len(pair) < 2:
+            q = rng.uniform(base.lower, base.upper).astype(np.float32)
+            if not sc.in_collision(q) and sc.min_distance(q) > 1e-3:
+                pair.append(q)
+        starts.append(pair[0])
+        goals.append(pair[1])
+    res = prrtc_plan_batch(np.stack(starts), np.stack(goals)[:, None, :], max_iterations=1000, step_size=0.6,
+                           num_new_samples=16, dynamic_domain=False, max_nodes=65536, min_vals=base.lower,
+                           max_vals=base.upper, collision_context=ctxs, launch=launch)
+    assert len(res) == 4
+    assert sum(r.solved for r in res) >= 3
+    for i, r in enumerate(res):
+        if not r.solved:
+            continue
+        path = r.path.cpu().numpy()
+        assert np.array_equal(path[0], starts[i]) and np.array_equal(path[-1], goals[i])
+        ok, md = orc.Scene(ctxs[i], base.dim).validate_path(path, 0.01)
+        assert ok, (i, md)
+        _check_tree_sound(orc.Scene(ctxs[i], base.dim), r.tree_a_configs.cpu().numpy(),
+                          r.tree_a_parents.cpu().numpy(), r.tree_a_size, base.dim)
