@@ -74,8 +74,9 @@ def parse():
     ap.add_argument("--tuning", default=None, metavar="E,T,CW[,R]",
                     help="skip the autotuner: explorers per problem, threads per explorer, waypoints per chunk, "
                          "CTAs per SM (0: as many as fit)")
-    ap.add_argument("--kernel", choices=["cc", "nn", "smooth"], default=None,
-                    help="run only the standalone FK+collision (cc), nearest-neighbour (nn) or smoothing adjoint (smooth) measurement")
+    ap.add_argument("--kernel", choices=["cc", "checkers", "nn", "smooth"], default=None,
+                    help="run only the standalone FK+collision (cc), per-checker (checkers), nearest-neighbour (nn) or "
+                         "smoothing adjoint (smooth) measurement")
     return ap.parse_args()
 
 
@@ -520,6 +521,7 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     out["batched_vs_plain"] = line["value"] / max(out["plain_per_problem"]["plans_per_s"], 1e-9)
 
     out.update(measure_cc(torch, dev, fp32))
+    out.update(measure_checkers(torch, dev))
     out.update(measure_nn(torch, dev, peaks))
     out.update(measure_smooth(torch, dev))
 
@@ -677,6 +679,40 @@ def measure_smooth(torch, dev, paths: int = 512, waypoints: int = 64, launches: 
                                "pairs_per_waypoint": pairs}}
 
 
+def measure_checkers(torch, dev, configs: int = 1 << 20, reps: int = 3):
+    """Batched collision checks per second of each checker the planner offers
+    (binary, differentiable, binary_coarse, binary_coarse_coop), with early
+    exit as the planner uses them, on the tabletop scene with uniformly
+    random configurations (the reference's benchmark_collision_checkers.py
+    compares the same checkers)."""
+    from prrtc_b200 import scenes
+    from prrtc_b200.collision import CollisionChecker
+    from prrtc_b200.context import build_collision_context
+
+    rng = np.random.default_rng(0)
+    ctx = build_collision_context(scenes.arm(0), scenes.tabletop_world(rng))
+    q = torch.from_numpy(rng.uniform(-2.8, 2.8, (configs, 7)).astype(np.float32)).to(dev)
+    outv = torch.empty(configs, dtype=torch.int32, device=dev)
+    res = {}
+    for name in ("binary", "differentiable", "binary_coarse", "binary_coarse_coop"):
+        chk = CollisionChecker(ctx, 7, name, 0.02, dev)
+        chk.check(q, out=outv)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            chk.check(q, out=outv)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        res[name] = {"checks_per_s": configs / (best * 1e-3),
+                     "in_collision": float(outv.float().mean().item())}
+        del chk
+    return {"cc_checkers": {"workload": f"tabletop scene, {configs} uniform random configurations, early exit",
+                            **res}}
+
+
 def measure_nn(torch, dev, peaks, reps: int = 3, launches: int = 20):
     """Standalone nearest neighbour (the prrtc_b200_nearest_neighbor entry of
     prrtc_nearest_neighbor) in two regimes: one query over a 32M-node tree
@@ -750,6 +786,8 @@ def run_kernel(a):
         out = measure_cc(torch, dev, fp32_peak_tflops(torch, lib, dev))
     elif a.kernel == "smooth":
         out = measure_smooth(torch, dev)
+    elif a.kernel == "checkers":
+        out = measure_checkers(torch, dev)
     else:
         out = measure_nn(torch, dev, measured_peaks())
     print(json.dumps(out))
