@@ -317,6 +317,14 @@ size_t prrtc_b200_check_configs_workspace_size(const prrtc_robot_t* robot, const
     return blob_stride(make_pack(*robot, *world, 1, 0, 0.0f));
 }
 
+// The batched checker sweeps every obstacle for the flat checkers (binary,
+// differentiable) even when early exit is allowed: the verdicts are the same,
+// and the full sweep measured faster (471 vs 405 M checks/s on 2^20 random
+// tabletop configurations, 79% in collision: most work items run before a
+// configuration's first hit is known).  The coarse-gated checkers keep early
+// exit (393 vs 385 M checks/s).
+static int32_t batch_sweep(int32_t mode, int32_t full_sweep) { return (full_sweep || mode == 0 || mode == 1) ? 1 : 0; }
+
 int prrtc_b200_check_configs(const prrtc_robot_t* robot, const prrtc_world_t* world, int32_t dim,
                              const float* configs, int32_t n, int32_t mode, float margin, int32_t full_sweep,
                              int32_t* verdicts, void* ws, size_t ws_bytes, void* stream) {
@@ -332,7 +340,8 @@ int prrtc_b200_check_configs(const prrtc_robot_t* robot, const prrtc_world_t* wo
     unsigned char* blob = static_cast<unsigned char*>(ws);
     cudaError_t e = launch_pack(s, 1, blob, stride, st);
     if (e != cudaSuccess) return cuda_fail(e);
-    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, configs, n, full_sweep, verdicts,
+    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, configs, n,
+                     batch_sweep(mode, full_sweep), verdicts,
                      st);
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
@@ -398,7 +407,8 @@ int prrtc_b200_check_edges(const prrtc_robot_t* robot, const prrtc_world_t* worl
     int32_t* verdicts = reinterpret_cast<int32_t*>(blob + stride);
     cudaError_t e = launch_pack(s, 1, blob, stride, st);
     if (e != cudaSuccess) return cuda_fail(e);
-    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, edges, n_edges * G, 0, verdicts,
+    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, edges, n_edges * G,
+                     batch_sweep(mode, 0), verdicts,
                      st, &pc);
     if (e != cudaSuccess) return cuda_fail(e);
     e = launch_edge_reduce(verdicts, n_edges, G, free_flags, st);
@@ -519,7 +529,8 @@ int prrtc_b200_check_configs_noalloc(const prrtc_robot_t* robot, const prrtc_wor
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = launch_pack(s, 1, blob, stride, st);
     if (e != cudaSuccess) return cuda_fail(e);
-    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, configs, n, full_sweep, verdicts,
+    e = launch_check(blob, (int)stride, world->self_pairs, s.J, s.S, s.K, s.Q, dim, configs, n,
+                     batch_sweep(mode, full_sweep), verdicts,
                      st);
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
