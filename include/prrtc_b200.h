@@ -251,7 +251,10 @@ int prrtc_b200_iteration(float* tree_a_configs, float* tree_b_configs, int32_t* 
 
 /* Collision verdicts of n configurations [n,dim] (1 = in collision) with the
  * checker of `collision_mode`.  full_sweep != 0 evaluates every pair with no
- * early exit (same verdicts; used to measure the kernel's FP32 throughput). */
+ * early exit (same verdicts; used to measure the kernel's FP32 throughput);
+ * the flat checkers (modes 0 and 1) sweep fully either way, which measured
+ * faster than their early exit, and the coarse-gated ones (2, 3) exit early
+ * unless full_sweep is set. */
 size_t prrtc_b200_check_configs_workspace_size(const prrtc_robot_t* robot, const prrtc_world_t* world);
 int prrtc_b200_check_configs(const prrtc_robot_t* robot, const prrtc_world_t* world, int32_t dim,
                              const float* configs, int32_t n, int32_t collision_mode,

@@ -2,8 +2,10 @@
 plan (scene packing, output initialisation, persistent planner, path
 extraction) replayable as one captured CUDA graph.
 
-Problems of different capacities go to separate ``BatchPlanner`` instances, one
-per ``max_nodes`` bucket, each with its own graph (``plan_buckets``).
+Problems of different tree capacities share one planner when ``max_nodes`` is
+a per-problem list (row stride = the largest capacity, each tree bounded by its
+own); separate ``BatchPlanner`` instances per capacity bucket, each with its
+own graph (``plan_buckets``), remain available.
 """
 from __future__ import annotations
 
