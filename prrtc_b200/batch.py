@@ -5,7 +5,7 @@ extraction) replayable as one captured CUDA graph.
 Problems of different tree capacities share one planner when ``max_nodes`` is
 a per-problem list (row stride = the largest capacity, each tree bounded by its
 own); separate ``BatchPlanner`` instances per capacity bucket, each with its
-own graph (``plan_buckets``), remain available.
+own graph (problems grouped by ``bucket_problems``), remain available.
 """
 from __future__ import annotations
 
