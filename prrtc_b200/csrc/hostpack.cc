@@ -191,6 +191,11 @@ PyObject* fill(PyObject*, PyObject* args) {
         if (is_shared) {
             const Table& a = tabs.t.empty() ? Table{} : tabs.t[0];
             const Py_ssize_t n = a.rows * row_bytes;
+            if (a.rows != mx) {  // the table changed since scan(): its reserved region no longer fits
+                PyErr_SetString(PyExc_ValueError, "a shared table's row count differs from the layout's");
+                ok = false;
+                break;
+            }
             if (toff < 0 || toff + n > ob.len) {
                 PyErr_SetString(PyExc_ValueError, "staging buffer too small");
                 ok = false;
