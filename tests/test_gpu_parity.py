@@ -546,3 +546,36 @@ def test_batch_mixed_full_and_trimmed_contexts(cuda, orc, launch):
         assert ok, (i, md)
         _check_tree_sound(orc.Scene(ctxs[i], base.dim), r.tree_a_configs.cpu().numpy(),
                           r.tree_a_parents.cpu().numpy(), r.tree_a_size, base.dim)
+
+
+def test_batch_inputs_as_device_tensors_and_tensor_contexts(cuda, orc):
+    """The batch call with its configurations and limits already on the
+    device (no copy) and per-problem contexts holding CPU torch tensors (no
+    buffer protocol, so the Python packer runs instead of the native one)
+    solves and re-validates like the same call with numpy inputs, which goes
+    through the native packer."""
+    from prrtc_b200 import prrtc_plan_batch
+
+    probs = [make_problem("uneven", 500 + i) for i in range(6)]
+    dim = probs[0].dim
+    G = max(p.goals.shape[0] for p in probs)
+    goals = np.zeros((len(probs), G, dim), np.float32)
+    for i, p in enumerate(probs):
+        goals[i, : p.goals.shape[0]] = p.goals
+    starts = np.stack([p.start for p in probs])
+    kw = dict(max_iterations=5000, num_new_samples=8, max_nodes=16384, collision_checker="binary_coarse_coop",
+              goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01, return_trees=False)
+    ref = prrtc_plan_batch(starts, goals, min_vals=probs[0].lower, max_vals=probs[0].upper,
+                           collision_context=[p.context for p in probs], **kw)
+    tctx = [{k: (torch.from_numpy(np.asarray(v)) if isinstance(v, np.ndarray) else v) for k, v in p.context.items()}
+            for p in probs]
+    res = prrtc_plan_batch(torch.from_numpy(starts).to(cuda), torch.from_numpy(goals).to(cuda),
+                           min_vals=torch.from_numpy(np.asarray(probs[0].lower, np.float32)).to(cuda),
+                           max_vals=torch.from_numpy(np.asarray(probs[0].upper, np.float32)).to(cuda),
+                           collision_context=tctx, **kw)
+    assert len(res) == len(ref) == len(probs)
+    assert sum(r.solved for r in res) >= len(probs) - 1
+    for p, r in zip(probs, res):
+        if r.solved:
+            ok, md = orc.Scene(p.context, dim).validate_path(r.path.cpu().numpy(), 0.01)
+            assert ok, md
