@@ -579,3 +579,36 @@ def test_batch_inputs_as_device_tensors_and_tensor_contexts(cuda, orc):
         if r.solved:
             ok, md = orc.Scene(p.context, dim).validate_path(r.path.cpu().numpy(), 0.01)
             assert ok, md
+
+
+@pytest.mark.parametrize("balance_mode,tree_ratio", [(0, 0.5), (2, 0.3), (3, 0.5)])
+def test_plan_balance_modes(cuda, orc, balance_mode, tree_ratio):
+    """Every tree-side rule of prrtc_planner.cu:790-824 (0: half the explorers
+    per tree, 1: size ratio -- the default, tested throughout --, 2: the
+    VAMP-style toggle, other: the smaller tree) plans and re-validates, in the
+    single-plan and the batched launch."""
+    from prrtc_b200 import prrtc_plan, prrtc_plan_batch
+
+    pr = make_problem("tabletop", 21)
+    sc = orc.Scene(pr.context, pr.dim)
+    r = prrtc_plan(pr.start, pr.goals, max_iterations=4000, num_new_samples=32, max_nodes=65536,
+                   balance_mode=balance_mode, tree_ratio=tree_ratio, min_vals=pr.lower, max_vals=pr.upper,
+                   collision_context=pr.context, collision_checker="binary_coarse_coop", edge_resolution=0.01)
+    assert r.solved
+    ok, md = sc.validate_path(r.path.cpu().numpy(), 0.01)
+    assert ok, md
+    probs = [make_problem("uneven", 600 + i) for i in range(4)]
+    G = max(p.goals.shape[0] for p in probs)
+    goals = np.zeros((len(probs), G, pr.dim), np.float32)
+    for i, p in enumerate(probs):
+        goals[i, : p.goals.shape[0]] = p.goals
+    res = prrtc_plan_batch(np.stack([p.start for p in probs]), goals, max_iterations=4000, num_new_samples=4,
+                           max_nodes=16384, balance_mode=balance_mode, tree_ratio=tree_ratio,
+                           min_vals=probs[0].lower, max_vals=probs[0].upper,
+                           collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
+                           goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01, return_trees=False)
+    assert sum(x.solved for x in res) >= len(probs) - 1
+    for p, x in zip(probs, res):
+        if x.solved:
+            ok, md = orc.Scene(p.context, pr.dim).validate_path(x.path.cpu().numpy(), 0.01)
+            assert ok, md
