@@ -612,3 +612,33 @@ def test_plan_balance_modes(cuda, orc, balance_mode, tree_ratio):
         if x.solved:
             ok, md = orc.Scene(p.context, pr.dim).validate_path(x.path.cpu().numpy(), 0.01)
             assert ok, md
+
+
+@pytest.mark.parametrize("launch", ["single", "persistent", "per_problem"])
+def test_unsolvable_problem_ends_at_max_iterations(cuda, orc, launch):
+    """A start configuration in collision makes the problem unsolvable (every
+    connect toward the start tree ends on a colliding waypoint).  Each
+    explorer then stops once its iteration count passes max_iterations
+    (prrtc_planner.cu:770-780): not solved, no path, and the reported
+    iteration count is max_iterations + 1, as in the oracle."""
+    from prrtc_b200 import prrtc_plan, prrtc_plan_batch
+
+    pr = make_problem("spheres16", 31)
+    sc = orc.Scene(pr.context, pr.dim)
+    rng = np.random.default_rng(31)
+    while True:
+        bad = rng.uniform(pr.lower, pr.upper).astype(np.float32)
+        if sc.in_collision(bad) and sc.min_distance(bad) < -0.02:
+            break
+    max_it = 150
+    ora = orc.plan(sc, bad, pr.goals[:1], pr.lower, pr.upper, max_iterations=max_it, num_new_samples=8,
+                   max_nodes=65536)
+    assert ora.solved != 1
+    kw = dict(max_iterations=max_it, num_new_samples=8, max_nodes=65536, min_vals=pr.lower, max_vals=pr.upper)
+    if launch == "single":
+        r = prrtc_plan(bad, pr.goals[:1], collision_context=pr.context, **kw)
+    else:
+        r = prrtc_plan_batch(bad[None], pr.goals[:1][None], collision_context=[pr.context], launch=launch,
+                             tail_explorers=False, **kw)[0]
+    assert not r.solved and r.path is None
+    assert r.iterations == ora.iter_count == max_it + 1
