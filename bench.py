@@ -69,8 +69,8 @@ def parse():
                     help="one launch for every problem with per-problem tree capacities (merged), or one "
                          "launch per capacity bucket on concurrent streams (buckets)")
     ap.add_argument("--tune", choices=["joint", "bucket"], default="bucket",
-                    help="explorer counts tuned per bucket alone (default; measured 144 K vs 139-143 K plans/s) "
-                         "or with the buckets running together (joint)")
+                    help="with --launch buckets: explorer counts tuned per bucket alone (default; measured 144 K "
+                         "vs 139-143 K plans/s) or with the buckets running together (joint)")
     ap.add_argument("--tuning", default=None, metavar="E,T,CW[,R]",
                     help="skip the autotuner: explorers per problem, threads per explorer, waypoints per chunk, "
                          "CTAs per SM (0: as many as fit)")
@@ -331,7 +331,8 @@ def run_ours(a):
         for st in streams:
             main.wait_stream(st)
 
-    # warm-up: first eager (validates), then capture one graph per bucket
+    # warm-up: first eager (validates), then capture one graph per planner (one
+    # planner for all problems by default, one per bucket with --launch buckets)
     for i in range(max(a.warmup, 1)):
         if i == 1 and not a.eager:
             for pl in planners.values():
