@@ -642,3 +642,66 @@ def test_unsolvable_problem_ends_at_max_iterations(cuda, orc, launch):
                              tail_explorers=False, **kw)[0]
     assert not r.solved and r.path is None
     assert r.iterations == ora.iter_count == max_it + 1
+
+
+def _long_chain_robot():
+    """A 12-dof arm in which every revolute joint is followed by two fixed
+    joints (identity transforms): 36 joints, past the 32 that the in-register
+    FK covers, so the checker takes its joint-parallel / chain-serial path."""
+    from prrtc_b200 import scenes
+    from prrtc_b200.context import RobotModel
+
+    base = scenes.arm(0, 12)
+    J0 = base.n_joints if hasattr(base, "n_joints") else base.twists.shape[0]
+    twists, ptf, parent, act = [], [], [], []
+    ident = np.array([1, 0, 0, 0, 0, 0, 0], np.float32)
+    for j in range(J0):
+        for k in range(3):
+            twists.append(base.twists[j] if k == 0 else np.zeros(6, np.float32))
+            ptf.append(base.parent_tf[j] if k == 0 else ident)
+            parent.append(len(parent) - 1)
+            act.append(int(base.act_idx[j]) if k == 0 else -1)
+    J = len(parent)
+    frame_map = {j: 3 * j + 2 for j in range(J0)}
+    return RobotModel(
+        twists=np.stack(twists).astype(np.float32), parent_tf=np.stack(ptf).astype(np.float32),
+        parent_idx=np.asarray(parent, np.int32), act_idx=np.asarray(act, np.int32),
+        mimic_mul=np.ones(J, np.float32), mimic_off=np.zeros(J, np.float32),
+        mimic_act_idx=np.full(J, -1, np.int32), topo_inv=np.arange(J, dtype=np.int32),
+        lower=base.lower, upper=base.upper,
+        sphere_frame=np.asarray([frame_map[int(f)] for f in base.sphere_frame], np.int32),
+        sphere_local=base.sphere_local, sphere_radius=base.sphere_radius,
+        link_pairs=[(frame_map[i], frame_map[j]) for i, j in base.link_pairs])
+
+
+def test_more_than_32_joints(cuda, orc):
+    """Robots past 32 joints: FK within 1e-5 of float64, checker verdicts equal
+    to the oracle's away from contact (flat and coarse checkers), and a plan
+    that re-validates."""
+    from prrtc_b200 import prrtc_plan, scenes
+    from prrtc_b200.collision import CollisionChecker, forward_kinematics
+
+    rob = _long_chain_robot()
+    assert rob.twists.shape[0] == 36
+
+    def checker(cfg, ctx):
+        return orc.Scene(ctx, cfg.shape[1]).check_configs(cfg, 0)
+
+    pr = scenes.make_problem("spheres16", 41, checker, robot=rob)
+    sc = orc.Scene(pr.context, pr.dim)
+    rng = np.random.default_rng(41)
+    q = rng.uniform(pr.lower, pr.upper, (300, pr.dim)).astype(np.float32)
+    F = forward_kinematics(q[:50], pr.context).cpu().numpy()
+    for i in range(50):
+        ref = sc.fk(q[i].astype(np.float64))
+        assert np.abs(F[i, :, 9:] - ref[:, 9:]).max() < 1e-5
+    far = np.abs(sc.min_distances(q)) > 1e-4
+    for mode, name in ((0, "binary"), (2, "binary_coarse"), (3, "binary_coarse_coop")):
+        v = CollisionChecker(pr.context, pr.dim, name, 0.02, cuda).check(q).cpu().numpy()
+        assert np.array_equal(v[far], sc.check_configs(q, mode)[far]), name
+    r = prrtc_plan(pr.start, pr.goals, max_iterations=5000, num_new_samples=32, max_nodes=65536,
+                   min_vals=pr.lower, max_vals=pr.upper, collision_context=pr.context,
+                   collision_checker="binary_coarse_coop", edge_resolution=0.02)
+    assert r.solved
+    ok, md = sc.validate_path(r.path.cpu().numpy(), 0.02)
+    assert ok, md
