@@ -290,3 +290,27 @@ def test_native_host_packer_random_contexts():
                 for i in range(B):
                     assert np.array_equal(got[i, :n[i]], ref[i, :n[i]]), (seed, key, i)
         assert (buf[total:] == 0x5A).all()
+
+
+def test_lpt_order_from_packed_counts_equals_lpt_order():
+    """The batch call orders problems by the row counts the packer already has
+    (_lpt_from_counts); that order equals lpt_order over the contexts, shared
+    tables (same cost for every problem) left out."""
+    from prrtc_b200.prrtc import _PACK_SPECS, _lpt_from_counts, _pack_worlds, _shared_table, lpt_order
+
+    rng = np.random.default_rng(9)
+    for trial in range(10):
+        B = int(rng.integers(1, 60))
+        ctxs = []
+        shared_half = np.zeros((1, 6), np.float32)
+        for i in range(B):
+            c = {"world_spheres": np.zeros((int(rng.integers(0, 5)), 4), np.float32),
+                 "world_boxes": np.zeros((int(rng.integers(0, 4)), 15), np.float32),
+                 "world_halfspaces": shared_half}
+            if rng.random() < 0.3:
+                c["world_capsules"] = np.zeros((int(rng.integers(0, 3)), 7), np.float32)
+            ctxs.append(c if rng.random() > 0.05 else None)
+        keys = [k for k, _, _ in _PACK_SPECS]
+        sh = {k: _shared_table(ctxs, k) for k in keys}
+        _, counts = _pack_worlds(ctxs, B, skip={k for k in keys if sh[k] is not None})
+        assert np.array_equal(_lpt_from_counts(counts, B), lpt_order(ctxs))
