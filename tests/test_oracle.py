@@ -323,7 +323,7 @@ def test_point_cloud_stage_brute_force(orc, arm):
     assert 0 < v.sum() < q.shape[0]
 
 
-@pytest.mark.parametrize("kind,seed", [("tabletop", 3), ("spheres16", 1), ("uneven", 7)])
+@pytest.mark.parametrize("kind,seed", [("tabletop", 3), ("spheres16", 1), ("uneven", 7), ("large", 5)])
 def test_autodiff_reference_matches_oracle_cost_and_differences(orc, kind, seed):
     """The autograd restatement of the smoothing cost (the stand-in for a
     jax.grad reference) agrees with the C oracle's cost, and its gradient with
@@ -338,7 +338,7 @@ def test_autodiff_reference_matches_oracle_cost_and_differences(orc, kind, seed)
     c64 = sc.smooth_cost(w, 0.02, 50.0, 1.0)
     assert abs(c - c64) <= 1e-9 * max(1.0, abs(c64))
     h = 1e-5
-    for i, d in [(1, 0), (2, 3), (4, 6), (3, 1)]:
+    for i, d in [(1, 0), (2, 3), (4, 6), (3, 1), (2, pr.dim - 1)]:
         wp, wm = w.copy(), w.copy()
         wp[i, d] += h
         wm[i, d] -= h
