@@ -113,3 +113,22 @@ def test_smoothing_pass_revalidates_or_reverts(cuda, orc):
         assert np.allclose(out[p][0], paths[p][0]) and np.allclose(out[p][-1], paths[p][-1])
     assert bool(accepted.any())
     assert bool((c1[accepted] <= c0[accepted] + 1e-3).all())
+
+
+def test_adjoint_mimic_dual_arm(cuda, orc):
+    """The adjoint through mimic joints (the dual arm: 14 actuated values, 18
+    joints, four mimic finger joints) against torch.autograd of the float64
+    restatement, on a straight-line path with small perturbations."""
+    from oracle.smooth_autodiff import smooth_grad
+    from prrtc_b200.smoothing import SmoothContext
+
+    pr = make_problem("large", 5)
+    rng = np.random.default_rng(5)
+    w = (np.linspace(pr.start, pr.goals[0], 12) + rng.normal(0, 0.03, (12, pr.dim))).astype(np.float32)
+    sctx = SmoothContext(pr.context, pr.dim, MARGIN, BETA, WLEN, cuda)
+    cost, grad = sctx.cost_grad(torch.from_numpy(w)[None].to(cuda))
+    c_ad, g_ad = smooth_grad(pr.context, w.astype(np.float64), MARGIN, BETA, WLEN)
+    assert abs(cost.item() - c_ad) <= 1e-4 * max(1.0, abs(c_ad))
+    g = grad[0].cpu().numpy().astype(np.float64)
+    rel = np.linalg.norm(g - g_ad) / np.linalg.norm(g_ad)
+    assert rel < 1e-3, rel
