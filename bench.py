@@ -77,6 +77,13 @@ def parse():
     ap.add_argument("--kernel", choices=["cc", "checkers", "nn", "smooth"], default=None,
                     help="run only the standalone FK+collision (cc), per-checker (checkers), nearest-neighbour (nn) or "
                          "smoothing adjoint (smooth) measurement")
+    ap.add_argument("--configs", default="1,2,4,5,dense",
+                    help="comma list of the extra workloads to measure on rank 0 after the headline: 1 (single plan, "
+                         "GPU and CPU path), 2 (1000 tabletop plans), 4 (smoothing of config-2 paths), 5 (1024 "
+                         "dual-arm plans + smoothing), dense (the 512-problem batch at the 16-sphere scene's "
+                         "density); 'none' skips them")
+    ap.add_argument("--config5-problems", type=int, default=1024)
+    ap.add_argument("--config2-problems", type=int, default=1000)
     return ap.parse_args()
 
 
@@ -240,26 +247,36 @@ def run_reference(a):
 
 # ----------------------------------------------------------------------------- our arm
 
-def fp32_peak_tflops(torch, lib, dev):
+def fp32_probe_rates(torch, lib, dev):
+    """FP32 FMA throughput of the two probes: scalar FFMA chains and packed
+    fma.rn.f32x2 chains (TFLOP/s, best of five launches each)."""
     from prrtc_b200 import _lib as L
 
     sm = torch.cuda.get_device_properties(dev).multi_processor_count
     sink = torch.zeros(sm * 8, device=dev)
     blocks, threads, iters = sm * 8, 256, 4096
     s = torch.cuda.current_stream().cuda_stream
-    L.check(lib.prrtc_b200_fp32_probe(blocks, threads, 64, sink.data_ptr(), s), "probe")
-    torch.cuda.synchronize()
-    best = 0.0
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        L.check(lib.prrtc_b200_fp32_probe(blocks, threads, iters, sink.data_ptr(), s), "probe")
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        flops = 2.0 * 8 * 16 * iters * blocks * threads
-        best = max(best, flops / (ms * 1e-3) / 1e12)
-    return best
+    rates = {}
+    for name, fn, per_iter in (("ffma", lib.prrtc_b200_fp32_probe, 2.0 * 8 * 16),
+                               ("ffma2", lib.prrtc_b200_fp32x2_probe, 4.0 * 8 * 16)):
+        L.check(fn(blocks, threads, 64, sink.data_ptr(), s), "probe")
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            L.check(fn(blocks, threads, iters, sink.data_ptr(), s), "probe")
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = max(best, per_iter * iters * blocks * threads / (ms * 1e-3) / 1e12)
+        rates[name] = best
+    return rates
+
+
+def fp32_peak_tflops(torch, lib, dev):
+    """FP32 roofline denominator: the faster of the scalar and packed FMA probes."""
+    return max(fp32_probe_rates(torch, lib, dev).values())
 
 
 def measured_peaks():
@@ -401,14 +418,16 @@ def run_ours(a):
         "success_rate": success,
         "p50_solve_ms": float(np.median(solve_ms)) if solve_ms.size else None,
     }
-    line["gpu_launches"] = 5 * len(planners) * a.steps  # per planner: pack, init, explore, finalize, paths
+    line["gpu_launches"] = 6 * len(planners) * a.steps  # per planner: fill, pack, init, explore, finalize, paths
+    if rank == 0 and not a.no_extras:
+        line.update(revalidate_step(planners))
 
     # e2e on every rank (each its own problems), whole job = all ranks' plans
     # over the slowest rank's seconds
     if not a.no_extras:
         if ws > 1:
             dist.barrier()
-        e_solved, e_s, e_h2d, e_d2h, e_steps = measure_e2e(torch, dev, planners, settings, tuned, cap_of)
+        e_solved, e_s, e_h2d, e_d2h, e_steps = measure_e2e(torch, dev, planners, settings, tuned, cap_of, a.steps)
         if ws > 1:
             v = torch.tensor([e_s, float(e_solved), float(e_h2d), float(e_d2h)], dtype=torch.float64, device=dev)
             vmax = v[:1].clone()
@@ -426,6 +445,7 @@ def run_ours(a):
 
     if rank == 0 and not a.no_extras:
         line.update(extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of))
+        line.update(measure_configs(a, torch, lib, dev, settings, tuned))
     if rank == 0:
         line["clocks"] = clk.summary()
         print(json.dumps(line))
@@ -448,8 +468,10 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
 
     out = {}
     peaks = measured_peaks()
-    fp32 = fp32_peak_tflops(torch, lib, dev)
+    rates = fp32_probe_rates(torch, lib, dev)
+    fp32 = max(rates.values())
     out["fp32_peak_tflops_measured"] = fp32
+    out["fp32_probe_tflops"] = rates
 
     # --- planner roofline: one instrumented (stats) eager step, events around each planner call
     flops = cfgs = edges = nn_nodes = 0
@@ -514,12 +536,14 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     solved_plain = plain(problems)
     torch.cuda.synchronize()
     dtp = time.perf_counter() - t0
-    out["plain_per_problem"] = {"plans_per_s": solved_plain / dtp, "success_rate": solved_plain / len(problems),
-                                "p50_solve_ms": float(np.median(plain_ms)) if plain_ms else None,
-                                "note": "one plain planner launch per problem over 8 streams, 128 explorers each, "
-                                        "host-timed incl. per-problem set-up (the reference's batch form); "
-                                        "second of two passes"}
+    out["plain_per_problem_e2e"] = {"plans_per_s": solved_plain / dtp, "success_rate": solved_plain / len(problems),
+                                    "p50_solve_ms": float(np.median(plain_ms)) if plain_ms else None,
+                                    "note": "one plain planner launch per problem over 8 streams, 128 explorers "
+                                            "each, host-timed incl. per-problem set-up (the reference's batch "
+                                            "form); second of two passes"}
+    out["plain_per_problem"] = measure_plain_device(torch, dev, problems, settings)
     out["batched_vs_plain"] = line["value"] / max(out["plain_per_problem"]["plans_per_s"], 1e-9)
+    out["batched_vs_plain_e2e"] = line["value"] / max(out["plain_per_problem_e2e"]["plans_per_s"], 1e-9)
 
     out.update(measure_cc(torch, dev, fp32))
     out.update(measure_checkers(torch, dev))
@@ -538,7 +562,38 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     return out
 
 
-def measure_e2e(torch, dev, planners, settings, tuned, cap_of):
+# ----------------------------------------------------------------------------- path re-validation
+
+def _validate_path(args):
+    ctx, dim, path = args
+    from oracle import oracle as O
+
+    ok, _ = O.Scene(ctx, dim).validate_path(path, 0.01)
+    return bool(ok)
+
+
+def revalidate_step(planners):
+    """Every path of the last timed step, re-validated after the timed region by
+    the float64 binary checker (the oracle, used here as the checker only) at
+    0.01 rad joint-space resolution, in a pool of spawned host processes."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+
+    jobs = []
+    for pl in planners.values():
+        for p, r in zip(pl.problems, pl.res.to_results(trees=False, paths_on_host=True)):
+            if r.solved:
+                jobs.append((p.context, p.dim, np.asarray(r.path)))
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(max(1, min(32, O.cpu_count()))) as pool:
+        ok = pool.map(_validate_path, jobs, chunksize=8)
+    return {"paths_revalidated": len(ok), "paths_failed": int(len(ok) - sum(ok)),
+            "revalidation": f"every solved path of the last timed step, float64 binary checker at 0.01 rad, "
+                            f"{time.perf_counter() - t0:.1f} s on the host after the timed region"}
+
+
+def measure_e2e(torch, dev, planners, settings, tuned, cap_of, steps):
     """End to end through the public API on this rank: host numpy inputs copied
     in and results plus paths copied back inside the timed region.  Returns
     (plans solved, seconds, host->device bytes per step, device->host bytes per
@@ -590,7 +645,7 @@ def measure_e2e(torch, dev, planners, settings, tuned, cap_of):
         collect(enqueue(k))
     torch.cuda.synchronize()
     _device.H2D_BYTES[0] = 0
-    k_e2e = 30
+    k_e2e = max(1, int(steps))
     solved = d2h = 0
     t0 = time.perf_counter()
     inflight = [enqueue(k) for k in range(min(depth - 1, k_e2e))]
@@ -780,6 +835,423 @@ def measure_nn(torch, dev, peaks, reps: int = 3, launches: int = 20):
             "nn_kernel_l2": {"workload": "64 queries x 4194304 nodes x 7 dims (117 MB tree, L2-resident)",
                              "ms": ms_l, "achieved_gbs": by_l / (ms_l * 1e-3) / 1e9,
                              "note": "each query re-reads the tree from L2, so the rate exceeds HBM peak"}}
+
+
+# ----------------------------------------------------------------------------- the other configurations
+
+def _wilson(k, n, z=1.96):
+    if n == 0:
+        return (0.0, 0.0)
+    p = k / n
+    d = 1 + z * z / n
+    c = (p + z * z / (2 * n)) / d
+    h = z * np.sqrt(p * (1 - p) / n + z * z / (4 * n * n)) / d
+    return (float(c - h), float(c + h))
+
+
+def _pad_goals(problems):
+    G = max(p.goals.shape[0] for p in problems)
+    goals = np.zeros((len(problems), G, problems[0].dim), np.float32)
+    for i, p in enumerate(problems):
+        goals[i, : p.goals.shape[0]] = p.goals
+    return goals, [p.goals.shape[0] for p in problems]
+
+
+def _timed_replays(torch, dev, pl, steps, warmup=2):
+    """Graph replays of one BatchPlanner, L2 flushed before each, CUDA events
+    around each replay; returns per-step ms."""
+    flush = torch.empty(int(256 * 2**20) // 4, dtype=torch.float32, device=dev)
+    for _ in range(warmup):
+        pl.run()
+    if pl.graph is None:
+        pl.capture()
+        pl.run()
+    torch.cuda.synchronize()
+    ms = []
+    for k in range(steps):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        pl.run()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    del flush
+    return ms
+
+
+def _batch_line(torch, dev, problems, caps, settings, steps, label):
+    """plans/s of one persistent batched launch (graph replay) over `problems`,
+    with success rate, tree sizes, device solve times and the nearest-neighbour
+    scan rate of one instrumented launch."""
+    from prrtc_b200.batch import STAT_NN_NODES, BatchPlanner
+
+    pl = BatchPlanner(problems, caps, settings, dev)
+    ms = _timed_replays(torch, dev, pl, steps)
+    blk = pl.summary_block().cpu().numpy()
+    solved = blk[:, 8] == 1
+    kt = blk[:, 9].copy().view(np.float32)
+    sizes = blk[:, 0:2].astype(np.int64)
+    res = pl.res.to_results(trees=False, paths_on_host=True)
+    pl.graph = None
+    del pl
+    ip = BatchPlanner(problems, caps, settings, dev, stats=True)
+    ip.launch()
+    torch.cuda.synchronize()
+    ip.stats.zero_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ip.launch()
+    e1.record()
+    e1.synchronize()
+    st = ip.stats.cpu().numpy()
+    nn_gbs = int(st[STAT_NN_NODES]) * problems[0].dim * 4 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    del ip
+    step_ms = float(np.mean(ms))
+    out = {"workload": label, "problems": len(problems), "steps": steps, "ms_per_step": step_ms,
+           "plans_per_s": float(solved.sum()) / (step_ms * 1e-3), "success_rate": float(solved.mean()),
+           "success_wilson95": _wilson(int(solved.sum()), len(problems)),
+           "unsolved": int((~solved).sum()),
+           "mean_tree_nodes": float(sizes.sum(1).mean()), "max_tree_nodes": int(sizes.sum(1).max()),
+           "p50_solve_ms": float(np.median(kt[solved])) if solved.any() else None,
+           "p95_solve_ms": float(np.percentile(kt[solved], 95)) if solved.any() else None,
+           "planner_nn_gbs": nn_gbs,
+           "buckets": {str(c): int(sum(1 for x in caps if x == c)) for c in sorted(set(caps))}}
+    return out, res
+
+
+def measure_dense(torch, dev, settings, steps=5, n=512):
+    """The 512-problem uneven batch at the 16-sphere scene's density (worlds in
+    [-0.8,0.8]^2 x [0,1.2], boxes of half extents up to 0.3 m): trees grow,
+    the capacity buckets fill and some problems are unsolvable (they run to
+    max_iterations and count as unsolved)."""
+    from prrtc_b200 import scenes
+    from prrtc_b200.collision import gpu_checker
+
+    robot = scenes.arm(0)
+    chk = gpu_checker(dev)
+    t0 = time.perf_counter()
+    problems = [scenes.make_problem("dense", 300000 + i, chk, robot=robot) for i in range(n)]
+    gen_s = time.perf_counter() - t0
+    out, _ = _batch_line(torch, dev, problems, [p.max_nodes for p in problems], settings, steps,
+                         "dense512: the uneven counts (4-128 spheres r 0.05-0.15, 0-32 boxes of half extents "
+                         "0.02-0.3 m) in [-0.8,0.8]^2 x [0,1.2], 1-8 goals, buckets 4096/16384/65536")
+    out["generation_s"] = gen_s
+    return {"dense512": out}
+
+
+def _pin_one_core():
+    os.sched_setaffinity(0, {sorted(os.sched_getaffinity(0))[0]})
+
+
+def _host_plan(args):
+    """One problem through the reference's host-driven RRT-Connect loop, restated
+    in C (prrtc_robogpu.py:103-298); returns (solved, seconds, config checks)."""
+    ctx, dim, start, goals, lo, hi, seed, threads = args
+    from oracle import oracle as O
+
+    sc = O.Scene(ctx, dim)
+    t0 = time.perf_counter()
+    r = O.rrtc_host_plan(sc, start, goals, lo, hi, max_iterations=1000, step_size=0.5, num_new_samples=128,
+                         granularity=16, max_nodes=65536, connect_max_steps=32, seed=seed, collision_mode=0,
+                         n_threads=threads)
+    return bool(r.solved), time.perf_counter() - t0, int(r.config_checks)
+
+
+def _cpu_run(problems, threads, budget_s, pin):
+    """The host loop over problems in order until the budget is spent, in one
+    spawned process (pinned to one core with `pin`)."""
+    import multiprocessing as mp
+
+    args = [(p.context, p.dim, p.start, p.goals, p.lower, p.upper, i, threads) for i, p in enumerate(problems)]
+    solved, secs, checks = [], [], 0
+    with mp.get_context("spawn").Pool(1, initializer=_pin_one_core if pin else None) as pool:
+        t0 = time.perf_counter()
+        for s, dt, c in pool.imap(_host_plan, args):
+            solved.append(s)
+            secs.append(dt)
+            checks += c
+            if time.perf_counter() - t0 > budget_s:
+                break
+    secs = np.asarray(secs)
+    ok = np.asarray(solved, bool)
+    return {"problems": int(ok.size), "threads": threads, "pinned_to_one_core": pin,
+            "success_rate": float(ok.mean()) if ok.size else None,
+            "p50_solve_ms": float(np.median(secs[ok]) * 1e3) if ok.any() else None,
+            "plans_per_s": float(ok.sum() / secs.sum()) if secs.size else None,
+            "checks_per_s": float(checks / secs.sum()) if secs.size else None}
+
+
+def measure_config1(torch, dev, n=32, cpu_budget_s=10.0):
+    """Single plan, 7-DOF arm among 16 spheres (seeds 0..n-1; the configuration
+    names seed 0), step 0.5, 128 samples, 10000 iterations, 65536 nodes, the
+    reference's defaults otherwise (binary checker, 16 waypoints per edge).  GPU:
+    one prrtc_plan call per problem -- device-clock solve time and the host wall
+    time of the call (inputs copied in, path read back).  CPU path: the
+    reference's host loop restated in C on this host, Run A on one pinned core,
+    Run B with a thread pool over each iteration's edge checks on every core."""
+    from oracle import oracle as O
+    from prrtc_b200 import prrtc_plan, scenes
+    from prrtc_b200.collision import gpu_checker
+
+    chk = gpu_checker(dev)
+    problems = [scenes.make_problem("spheres16", i, chk) for i in range(n)]
+    kw = dict(max_iterations=10000, step_size=0.5, num_new_samples=128, max_nodes=65536)
+    p0 = problems[0]
+    prrtc_plan(p0.start, p0.goals, min_vals=p0.lower, max_vals=p0.upper, collision_context=p0.context, **kw)
+    torch.cuda.synchronize()
+    dev_ms, wall_ms, ok = [], [], []
+    for p in problems:
+        t0 = time.perf_counter()
+        r = prrtc_plan(p.start, p.goals, min_vals=p.lower, max_vals=p.upper, collision_context=p.context, **kw)
+        path = r.path.cpu() if r.solved else None
+        wall_ms.append((time.perf_counter() - t0) * 1e3)
+        dev_ms.append(r.kernel_time_ms)
+        ok.append(bool(r.solved) and path is not None)
+    ok = np.asarray(ok)
+    gpu = {"problems": n, "success_rate": float(ok.mean()),
+           "p50_solve_ms_device": float(np.median(np.asarray(dev_ms)[ok])),
+           "p50_call_ms_host": float(np.median(np.asarray(wall_ms)[ok])),
+           "note": "device: globaltimer from the first explorer's start to the solution; host: the whole "
+                   "prrtc_plan call including set-up, copies and the path read-back"}
+    cores = O.cpu_count()
+    run_a = _cpu_run(problems, 1, cpu_budget_s, True)
+    run_b = _cpu_run(problems, cores, cpu_budget_s, False)
+    return {"config1_single_plan": {"workload": "7-DOF arm, 16 world spheres, 1 goal, seeds 0..%d" % (n - 1),
+                                    "gpu": gpu, "cpu_run_a": run_a, "cpu_run_b": run_b, "cpu": cpu_model(),
+                                    "cpu_path": "host-driven RRT-Connect (prrtc_robogpu.py:103-298) restated "
+                                                "in C: uniform samples, brute-force nearest neighbour, steer, "
+                                                "batched edge checks, greedy connect (JAX and PyRoFFI absent)"}}
+
+
+def measure_config2_4(torch, dev, settings, want4, n=1000, oracle_sample=100, smooth_paths_n=512):
+    """Config 2: n tabletop problems as plain single plans (one launch per
+    problem, 8 streams): success, path cost, device time to solution; the
+    oracle's sequential restatement of the planner on the first problems as the
+    reference.  Config 4: the first 512 solved paths resampled to 64 waypoints,
+    50 projected gradient steps of the adjoint cost (each path in its own
+    world, one batched launch per step), exact re-validation at 0.01 rad."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+    from prrtc_b200 import prrtc_plan_batch, scenes
+    from prrtc_b200.collision import gpu_checker
+
+    chk = gpu_checker(dev)
+    robot = scenes.arm(0)
+    t0 = time.perf_counter()
+    problems = [scenes.make_problem("tabletop", 200000 + i, chk, robot=robot) for i in range(n)]
+    gen_s = time.perf_counter() - t0
+    goals, gcount = _pad_goals(problems)
+    kw = dict(max_iterations=settings.max_iterations, num_new_samples=128, max_nodes=65536,
+              collision_checker=settings.collision_checker, edge_resolution=settings.edge_resolution)
+    t0 = time.perf_counter()
+    res = prrtc_plan_batch(np.stack([p.start for p in problems]), goals, goal_counts=gcount,
+                           min_vals=problems[0].lower, max_vals=problems[0].upper,
+                           collision_context=[p.context for p in problems], launch="per_problem",
+                           return_trees=False, **kw)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ok = np.array([r.solved for r in res])
+    cost = np.array([r.cost for r in res if r.solved])
+    kt = np.array([r.kernel_time_ms for r in res if r.solved])
+    # the oracle's sequential restatement (explorers in round-robin) on the first problems
+    jobs = [(p.context, p.dim, p.start, p.goals, p.lower, p.upper) for p in problems[:oracle_sample]]
+    with mp.get_context("spawn").Pool(max(1, min(32, O.cpu_count()))) as pool:
+        ora = pool.map(_oracle_plan_job, jobs, chunksize=2)
+    oo = np.array([s for s, _ in ora])
+    oc = np.array([c for s, c in ora if s])
+    out = {"config2_tabletop": {
+        "workload": f"{n} tabletop problems (floor, table + 3-5 shelves + clutter = 20 boxes, 8 capsules, "
+                    "32 spheres, 4 goals), plain single-plan launches, 128 explorers, 65536 nodes",
+        "problems": n, "generation_s": gen_s, "wall_s": wall, "success_rate": float(ok.mean()),
+        "success_wilson95": _wilson(int(ok.sum()), n),
+        "cost_mean": float(cost.mean()), "cost_median": float(np.median(cost)),
+        "p50_time_to_solution_ms": float(np.median(kt)), "p95_time_to_solution_ms": float(np.percentile(kt, 95)),
+        "oracle": {"problems": int(oo.size), "success_rate": float(oo.mean()),
+                   "success_wilson95": _wilson(int(oo.sum()), int(oo.size)),
+                   "cost_median": float(np.median(oc)) if oc.size else None,
+                   "gpu_cost_median_same_problems": float(np.median([r.cost for r in res[:oracle_sample]
+                                                                     if r.solved])),
+                   "what": "sequential restatement of the same planner (explorers in round-robin), same "
+                           "settings, on the first problems"}}}
+    if want4:
+        out.update(measure_config4(torch, dev, problems, res, smooth_paths_n))
+    return out
+
+
+def _oracle_plan_job(args):
+    ctx, dim, start, goals, lo, hi = args
+    from oracle import oracle as O
+
+    r = O.plan(O.Scene(ctx, dim), start, goals, lo, hi, max_iterations=10000, num_new_samples=128, max_nodes=65536,
+               collision_mode=3, edge_resolution=0.01)
+    return r.solved == 1, r.cost
+
+
+def _smoothing_pass(torch, dev, paths, contexts, lower, upper, waypoints, steps=50):
+    """Resample, `steps` projected gradient steps of the batched adjoint
+    (CUDA events around the steps), exact re-validation; wall time of the whole
+    pass."""
+    from prrtc_b200.smoothing import BatchSmoothContext, projected_steps, resample_path, revalidate_batch
+
+    t0 = time.perf_counter()
+    dim = int(np.asarray(paths[0]).shape[1])
+    init = torch.from_numpy(np.stack([resample_path(np.asarray(p), waypoints) for p in paths])).to(dev)
+    sctx = BatchSmoothContext(contexts, dim, device=dev)
+    c0, _ = sctx.cost_grad(init, need_grad=False)
+    projected_steps(sctx, init, lower, upper, 2, 0.05)  # warm
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    x = projected_steps(sctx, init, lower, upper, steps, 0.05)
+    e1.record()
+    e1.synchronize()
+    c1, _ = sctx.cost_grad(x, need_grad=False)
+    accepted = revalidate_batch(x, contexts, 0.01, dev)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    acc = accepted.cpu().numpy()
+    c0, c1 = c0.cpu().numpy(), c1.cpu().numpy()
+    final = np.where(acc, c1, c0)
+    return {"paths": len(paths), "waypoints": waypoints, "dim": dim, "steps": steps,
+            "device_ms_steps": e0.elapsed_time(e1), "ms_per_step": e0.elapsed_time(e1) / steps,
+            "wall_s_pass": wall, "accepted_rate": float(acc.mean()),
+            "cost_before_mean": float(c0.mean()), "cost_after_mean": float(final.mean()),
+            "cost_drop_mean": float((c0 - final).mean()),
+            "note": "cost = sum softplus_50(0.02 - d) over robot-sphere/world and self pairs + squared path "
+                    "length; paths that fail exact re-validation at 0.01 rad revert to the planner's path"}
+
+
+def measure_config4(torch, dev, problems, res, n=512):
+    solved = [(p, r) for p, r in zip(problems, res) if r.solved]
+    sel = solved[:n]
+    paths = [np.asarray(r.path.cpu() if hasattr(r.path, "cpu") else r.path) for _, r in sel]
+    out = _smoothing_pass(torch, dev, paths, [p.context for p, _ in sel], sel[0][0].lower, sel[0][0].upper, 64)
+    out["workload"] = f"the first {len(sel)} solved config-2 paths, 64 waypoints x 7 DOF, each in its own world"
+    return {"config4_smoothing": out}
+
+
+def measure_config5(torch, dev, settings, tuned, n=1024, steps=3):
+    """1024 dual-arm problems (two 7-DOF arms 0.6 m apart with two mimic finger
+    joints each, 120 spheres; 256 spheres + 64 boxes + floor; 1-4 goals; 131072
+    nodes) in one persistent batched launch, then the smoothing pass at 96
+    waypoints x 14 DOF on the solved paths."""
+    from prrtc_b200 import scenes
+    from prrtc_b200.batch import PlanSettings
+    from prrtc_b200.collision import gpu_checker
+
+    chk = gpu_checker(dev)
+    robot = scenes.dual_arm(0)
+    t0 = time.perf_counter()
+    problems = [scenes.make_problem("large", 400000 + i, chk, robot=robot) for i in range(n)]
+    gen_s = time.perf_counter() - t0
+    s = PlanSettings(**{**settings.__dict__, **tuned})
+    line, res = _batch_line(torch, dev, problems, [p.max_nodes for p in problems], s, steps,
+                            f"{n} dual-arm problems (14 DOF + 4 mimic joints, 120 spheres), 256 spheres + 64 boxes "
+                            "+ floor, 1-4 goals, 131072 nodes")
+    line["generation_s"] = gen_s
+    sel = [(p, r) for p, r in zip(problems, res) if r.solved]
+    sm = _smoothing_pass(torch, dev, [np.asarray(r.path) for _, r in sel], [p.context for p, _ in sel],
+                         sel[0][0].lower, sel[0][0].upper, 96)
+    return {"config5_dual_arm": {**line, "smoothing": sm}}
+
+
+def measure_plain_device(torch, dev, problems, settings, n_streams=8):
+    """The plain per-problem form timed on the device: every problem's inputs
+    staged on the GPU beforehand, one plain planner launch per problem (128
+    explorers, its own tree capacity) over `n_streams` streams, all launches
+    captured in one CUDA graph and replayed between CUDA events -- host set-up
+    excluded, as for the batched value."""
+    import ctypes as C
+
+    from prrtc_b200 import _lib
+    from prrtc_b200.device import DeviceContext, workspace
+    from prrtc_b200.prrtc import _attrs, _outputs_struct, _resolve_collision_mode, _tuning
+
+    lib = _lib.load()
+    keep, calls = [], []
+    mode = _resolve_collision_mode(settings.collision_checker)
+    for p in problems:
+        N = int(p.max_nodes)
+        ctx = DeviceContext(p.context, dev)
+        st = torch.from_numpy(p.start).to(dev)
+        gl = torch.from_numpy(np.ascontiguousarray(p.goals)).to(dev)
+        lo, hi = torch.from_numpy(p.lower).to(dev), torch.from_numpy(p.upper).to(dev)
+        inp = _lib.Inputs()
+        inp.start_config, inp.goal_configs, inp.num_goals = st.data_ptr(), gl.data_ptr(), gl.shape[0]
+        inp.min_vals, inp.max_vals = lo.data_ptr(), hi.data_ptr()
+        inp.robot, inp.world = ctx.robot(), ctx.world()
+        t = {k: torch.empty(shape, dtype=dt, device=dev) for k, shape, dt in (
+            ("ta", (p.dim, N), torch.float32), ("tb", (p.dim, N), torch.float32), ("pa", (N,), torch.int32),
+            ("pb", (N,), torch.int32), ("sz", (2,), torch.int32), ("cp", (2,), torch.int32),
+            ("it", (1,), torch.int32), ("cn", (3,), torch.int32), ("sv", (1,), torch.int32),
+            ("kt", (1,), torch.float32))}
+        outs = _outputs_struct(t["ta"], t["tb"], t["pa"], t["pb"], t["sz"], t["cp"], t["it"], t["cn"], t["sv"],
+                               t["kt"])
+        attrs = _attrs(settings.max_iterations, settings.step_size, 128, settings.balance_mode, settings.tree_ratio,
+                       settings.dynamic_domain, settings.dd_alpha, settings.dd_radius, settings.dd_min_radius, p.dim,
+                       N, settings.granularity, mode, settings.collision_margin)
+        tun = _tuning(settings.edge_resolution, 128, 16)
+        ws = workspace(lib.prrtc_b200_plan_workspace_size(C.byref(inp), C.byref(attrs), C.byref(tun)), dev)
+        keep.append((ctx, st, gl, lo, hi, t, ws))
+        calls.append((inp, outs, attrs, tun, ws, t))
+    streams = [torch.cuda.Stream(device=dev) for _ in range(n_streams)]
+
+    def launch_all():
+        main = torch.cuda.current_stream()
+        for s in streams:
+            s.wait_stream(main)
+        for i, (inp, outs, attrs, tun, ws, _) in enumerate(calls):
+            s = streams[i % n_streams]
+            _lib.check(lib.prrtc_b200_plan(C.byref(inp), C.byref(outs), C.byref(attrs), C.byref(tun), ws.data_ptr(),
+                                           ws.numel(), s.cuda_stream), "prrtc_b200_plan")
+        for s in streams:
+            main.wait_stream(s)
+
+    launch_all()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        launch_all()
+    flush = torch.empty(int(256 * 2**20) // 4, dtype=torch.float32, device=dev)
+    ms = []
+    for k in range(4):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        e1.synchronize()
+        if k:
+            ms.append(e0.elapsed_time(e1))
+    solved = np.array([int(c[5]["sv"].item()) == 1 for c in calls])
+    kt = np.array([float(c[5]["kt"].item()) for c in calls])
+    del g
+    step = float(np.mean(ms))
+    return {"plans_per_s": float(solved.sum()) / (step * 1e-3), "ms_per_step": step,
+            "success_rate": float(solved.mean()), "p50_solve_ms": float(np.median(kt[solved])),
+            "note": f"one plain planner launch per problem (128 explorers, per-problem tree capacity) over "
+                    f"{n_streams} streams, inputs resident, all launches in one CUDA graph replayed between "
+                    f"CUDA events, L2 flushed before each replay; mean of 3 replays"}
+
+
+def measure_configs(a, torch, lib, dev, settings, tuned):
+    """The other BASELINE configurations, rank 0, after the headline."""
+    want = set(x.strip() for x in a.configs.split(",")) - {"none", ""}
+    out = {}
+    tuned_one = next(iter(tuned.values()))
+    if "dense" in want:
+        from prrtc_b200.batch import PlanSettings
+
+        out.update(measure_dense(torch, dev, PlanSettings(**{**settings.__dict__, **tuned_one})))
+    if "1" in want:
+        out.update(measure_config1(torch, dev))
+    if "2" in want or "4" in want:
+        out.update(measure_config2_4(torch, dev, settings, "4" in want, n=a.config2_problems))
+    if "5" in want:
+        out.update(measure_config5(torch, dev, settings, tuned_one, n=a.config5_problems))
+    return out
 
 
 def run_kernel(a):

@@ -25,6 +25,10 @@
  *                                   (exposed as a batched primitive)
  *   prrtc_b200_fk / _halton      <- fk_single call sites (prrtc_planner.cu:509-522) and the
  *                                   Halton sampler (144-157, 747-788), exposed for parity tests
+ *   prrtc_b200_choose_tree       <- the planner's tree-side balance rule
+ *                                   (prrtc_planner.cu:790-824), exposed for parity tests
+ *   prrtc_b200_radius_update     <- prrtc_radius_shrink_atomic / prrtc_radius_grow_atomic
+ *                                   (prrtc_planner.cu:46-83), exposed for parity tests
  *   prrtc_b200_smooth_cost_grad  <- no reference counterpart: adjoint of the smooth
  *                                   collision + length cost for post-plan smoothing
  */
@@ -150,10 +154,8 @@ typedef struct {
 /* Extensions (all-zero = defaults). */
 typedef struct {
     float edge_resolution;       /* >0: an edge gets max(granularity, ceil(len/res)) waypoints */
-    int32_t threads_per_explorer;/* threads of one explorer: 64, 128 or 256 (one explorer per CTA,
-                                    default 128), or 32 (one explorer per warp; the batched
-                                    planner then runs 4 explorers of a problem per CTA, sharing
-                                    one staged scene) */
+    int32_t threads_per_explorer;/* threads of one explorer (one explorer per CTA): 32, 64, 128
+                                    or 256 (default 128) */
     int32_t waypoint_chunk;      /* waypoints checked per CTA pass: 8, 16 or 32 (default 16) */
     int32_t resident_ctas;       /* batched planner grid (default: all resident CTAs) */
     uint64_t* stats;             /* optional device counters [4], accumulated: edges checked,
@@ -271,9 +273,14 @@ int prrtc_b200_check_configs(const prrtc_robot_t* robot, const prrtc_world_t* wo
  * until process exit; a larger scene returns PRRTC_B200_ETOOLARGE before any
  * CUDA call.  The first call on a device resolves the array's device address
  * (cudaGetSymbolAddress) with that device current, so make that first call
- * before any stream capture.  Every call rewrites the whole array; calls that
- * overlap on the GPU (other streams or host threads on the same device) share
- * it and race -- serialise them. */
+ * before any stream capture; the address is kept per device and CUDA context,
+ * and a call in another context (a different driver context made current, or
+ * the primary context re-created after cudaDeviceReset) resolves it again, so
+ * that first call in a new context also belongs before any capture.  Every call
+ * rewrites the header and every section of the array that the checker reads,
+ * so nothing needs clearing between calls; calls that overlap on the GPU (other
+ * streams or host threads on the same device) share the array and race --
+ * serialise them. */
 #define PRRTC_B200_NOALLOC_SCENE_MAX (256 * 1024)
 int prrtc_b200_check_configs_noalloc(const prrtc_robot_t* robot, const prrtc_world_t* world, int32_t dim,
                                      const float* configs, int32_t n, int32_t collision_mode,
@@ -311,6 +318,24 @@ int prrtc_b200_fk(const prrtc_robot_t* robot, int32_t dim, const float* configs,
 int prrtc_b200_halton(int32_t explorer, int32_t n, int32_t dim, const float* min_vals,
                       const float* max_vals, float* samples, void* stream);
 
+/* The planner's tree-side rule (balance_mode 0-3) for n cases: explorer bid of
+ * nblocks (one CUDA block each) with tree sizes sizes[2c], sizes[2c+1] and
+ * iteration count local_iter[c] chooses tree_out[c*nblocks+bid] (0 = A, 1 = B);
+ * vamp_in / vamp_out [n, nblocks] carry an explorer's balance_mode-2 side
+ * before and after the choice. */
+int prrtc_b200_choose_tree(int32_t balance_mode, int32_t n, const int32_t* sizes,
+                           const int32_t* local_iter, const int32_t* vamp_in, int32_t nblocks,
+                           float tree_ratio, int32_t* tree_out, int32_t* vamp_out, void* stream);
+
+/* The planner's dynamic-domain radius updates on radii[] (FLT_MAX = unset):
+ * update i is op[i] (0 = shrink after a failed extension from node idx[i], 1 = grow
+ * after a successful one).  sequential = 0: one thread per update, so updates of
+ * one node contend on its compare-and-swap loop; sequential != 0: applied in order.
+ * err (optional, device int32): set to 1 if a loop's iteration guard ran out. */
+int prrtc_b200_radius_update(float* radii, const int32_t* idx, const int32_t* op, int32_t n,
+                             float dd_alpha, float dd_radius, float dd_min_radius,
+                             int32_t sequential, int32_t* err, void* stream);
+
 /* Root(A) -> connection -> root(B) paths of B solved problems ([B,...] planner
  * outputs) into paths [B,max_len,dim]; lengths [B] (0 when unsolved, -1 when
  * longer than max_len) and costs [B] (sum of segment norms). */
@@ -331,10 +356,26 @@ int prrtc_b200_smooth_cost_grad(const prrtc_robot_t* robot, const prrtc_world_t*
                                 float margin, float beta, float w_len, float* cost, float* grad,
                                 void* workspace, size_t workspace_bytes, void* stream);
 
+/* The same cost and gradient for the paths of a batch, path p [W,dim] of
+ * waypoints [batch,W,dim] against problem p's own world and self pairs, as
+ * prrtc_b200_plan_batch reads them from `in` (robot, batch, the per-problem world
+ * tables and counts; the start, goal, order and capacity fields are not used).
+ * No reference counterpart (post-plan smoothing of a batch plan's paths). */
+size_t prrtc_b200_smooth_batch_workspace_size(const prrtc_batch_inputs_t* in);
+int prrtc_b200_smooth_cost_grad_batch(const prrtc_batch_inputs_t* in, int32_t dim, const float* waypoints,
+                                      int32_t n_waypoints, float margin, float beta, float w_len,
+                                      float* cost, float* grad, void* workspace, size_t workspace_bytes,
+                                      void* stream);
+
 /* Diagnostic: FP32 FFMA throughput probe (blocks x threads, iters x 8 independent
  * FFMA chains per thread); sink receives one value per block so the work is live.
  * Used to measure the FP32 roofline denominator. */
 int prrtc_b200_fp32_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink, void* stream);
+
+/* Diagnostic: the same probe with packed FP32 FMAs (fma.rn.f32x2: iters x 8 chains
+ * of two lanes per thread, twice the flops of prrtc_b200_fp32_probe per iteration).
+ * The larger of the two rates is the FP32 roofline denominator. */
+int prrtc_b200_fp32x2_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink, void* stream);
 
 const char* prrtc_b200_error_string(int code);
 int prrtc_b200_last_cuda_error(void);

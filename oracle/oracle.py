@@ -100,6 +100,9 @@ def _declare(L: C.CDLL) -> None:
         "orc_extend": (None, [P, P, I, F, F, P]),
         "orc_edge_waypoints": (I, [P, I, I, F]),
         "orc_waypoint": (None, [P, P, I, I, I, P]),
+        "orc_choose_tree": (I, [I, I, I, I, I, I, F, P]),
+        "orc_radius_shrink": (None, [P, I, F, F, F]),
+        "orc_radius_grow": (None, [P, I, F]),
         "orc_fk_f64": (None, [P, P, P]),
         "orc_fk_f32": (None, [P, P, P]),
         "orc_config_in_collision": (I, [P, P, I, F]),
@@ -281,6 +284,37 @@ def extend(base, sample, nd: float, step: float) -> np.ndarray:
     out = np.zeros_like(b)
     lib().orc_extend(_ptr(b), _ptr(s), b.shape[0], float(np.float32(nd)), float(step), _ptr(out))
     return out
+
+
+def choose_tree(mode: int, sizes, local_iter, vamp_in, nblocks: int, tree_ratio: float):
+    """Tree side of every explorer bid < nblocks for n cases (sizes [n,2],
+    local_iter [n], vamp_in [n,nblocks]) -> (tree [n,nblocks], vamp [n,nblocks])."""
+    sizes = np.asarray(sizes, np.int32).reshape(-1, 2)
+    li = np.asarray(local_iter, np.int32).reshape(-1)
+    vin = np.asarray(vamp_in, np.int32).reshape(sizes.shape[0], nblocks)
+    tree = np.zeros_like(vin)
+    vout = np.zeros_like(vin)
+    fn = lib().orc_choose_tree
+    for c in range(sizes.shape[0]):
+        for b in range(nblocks):
+            v = C.c_int(int(vin[c, b]))
+            tree[c, b] = fn(int(mode), int(li[c]), b, int(nblocks), int(sizes[c, 0]), int(sizes[c, 1]),
+                            float(tree_ratio), C.byref(v))
+            vout[c, b] = v.value
+    return tree, vout
+
+
+def radius_updates(radii, idx, op, alpha: float, r0: float, rmin: float) -> np.ndarray:
+    """Apply the dynamic-domain updates op[i] (0 shrink, 1 grow) on radii[idx[i]]
+    in order; returns the new float32 radii (FLT_MAX = unset)."""
+    r = np.array(radii, np.float32, copy=True)
+    L = lib()
+    for i, o in zip(np.asarray(idx).reshape(-1), np.asarray(op).reshape(-1)):
+        if int(o) == 0:
+            L.orc_radius_shrink(_ptr(r), int(i), float(alpha), float(r0), float(rmin))
+        else:
+            L.orc_radius_grow(_ptr(r), int(i), float(alpha))
+    return r
 
 
 def edge_waypoints(base, end, granularity: int, resolution: float = 0.0) -> np.ndarray:

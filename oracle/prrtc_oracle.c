@@ -486,22 +486,29 @@ typedef struct {
     int done;
 } Explorer;
 
-/* 46-65 */
-static void radius_shrink(float* radii, int idx, float alpha, float r0, float rmin) {
+/* 46-65 (prrtc_radius_shrink_atomic; one update at a time) */
+void orc_radius_shrink(float* radii, int idx, float alpha, float r0, float rmin) {
     const float old = radii[idx];
     radii[idx] = (old == FLT_MAX) ? r0 : fmaxf(old * (1.0f - alpha), rmin);
 }
 
-/* 67-83 */
-static void radius_grow(float* radii, int idx, float alpha) {
+/* 67-83 (prrtc_radius_grow_atomic) */
+void orc_radius_grow(float* radii, int idx, float alpha) {
     const float old = radii[idx];
     if (old != FLT_MAX) radii[idx] = old * (1.0f + alpha);
 }
 
+static void radius_shrink(float* radii, int idx, float alpha, float r0, float rmin) {
+    orc_radius_shrink(radii, idx, alpha, r0, rmin);
+}
+
+static void radius_grow(float* radii, int idx, float alpha) { orc_radius_grow(radii, idx, alpha); }
+
 /* 790-824 */
-static int choose_tree(Explorer* ex, int bid, int nblocks, const int sizes[2], int mode, float ratio_thr) {
-    const int size_a = sizes[0], size_b = sizes[1], total = size_a + size_b;
-    if (mode == 0 || ex->local_iter == 1) return (bid < (nblocks / 2)) ? 0 : 1;
+int orc_choose_tree(int mode, int local_iter, int bid, int nblocks, int size_a, int size_b, float ratio_thr,
+                    int* vamp) {
+    const int total = size_a + size_b;
+    if (mode == 0 || local_iter == 1) return (bid < (nblocks / 2)) ? 0 : 1;
     if (mode == 1) {
         const int diff = size_a >= size_b ? size_a - size_b : size_b - size_a;
         const float ratio = total > 0 ? (float)size_a / (float)total : 0.5f;
@@ -509,14 +516,18 @@ static int choose_tree(Explorer* ex, int bid, int nblocks, const int sizes[2], i
         return ratio < ratio_thr ? 0 : 1;
     }
     if (mode == 2) {
-        const int o_id = 1 - ex->vamp_tree;
-        const int t_sz = ex->vamp_tree == 0 ? size_a : size_b;
+        const int o_id = 1 - *vamp;
+        const int t_sz = *vamp == 0 ? size_a : size_b;
         const int o_sz = o_id == 0 ? size_a : size_b;
         const float r = t_sz > 0 ? fabsf((float)(t_sz - o_sz) / (float)t_sz) : 0.0f;
-        if (r < ratio_thr) ex->vamp_tree = 1 - ex->vamp_tree;
-        return ex->vamp_tree;
+        if (r < ratio_thr) *vamp = 1 - *vamp;
+        return *vamp;
     }
     return size_a <= size_b ? 0 : 1;
+}
+
+static int choose_tree(Explorer* ex, int bid, int nblocks, const int sizes[2], int mode, float ratio_thr) {
+    return orc_choose_tree(mode, ex->local_iter, bid, nblocks, sizes[0], sizes[1], ratio_thr, &ex->vamp_tree);
 }
 
 typedef struct {

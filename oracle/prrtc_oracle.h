@@ -117,6 +117,16 @@ int orc_edge_waypoints(const float* delta, int dim, int granularity, float resol
 /* waypoint k of G: base + ((k+1)/G) * delta, one fma per coordinate */
 void orc_waypoint(const float* base, const float* delta, int dim, int k, int G, float* out);
 
+/* Tree-side balance (prrtc_planner.cu:790-824): the tree (0 = A, 1 = B) explorer
+ * bid of nblocks extends, given the sizes and its iteration count; *vamp is the
+ * explorer's balance_mode-2 side, updated in place. */
+int orc_choose_tree(int mode, int local_iter, int bid, int nblocks, int size_a, int size_b, float ratio_thr,
+                    int* vamp);
+
+/* Dynamic-domain radius updates (prrtc_planner.cu:46-83), FLT_MAX = unset. */
+void orc_radius_shrink(float* radii, int idx, float alpha, float r0, float rmin);
+void orc_radius_grow(float* radii, int idx, float alpha);
+
 /* ---- forward kinematics: frames [J][12] = row-major R (9) then t (3), in the
  * output (original) frame order ---- */
 void orc_fk_f64(const OrcScene* sc, const double* q, double* frames);

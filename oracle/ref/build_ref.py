@@ -2,14 +2,16 @@
 
 The reference library cannot be built here as a whole: its handlers need XLA's
 FFI headers (jaxlib is absent) and its collision/FK device functions come from
-PyRoFFI (absent).  The sampling, nearest-neighbour, extend, waypoint and connect
-arithmetic of its planner does not depend on either, so this recipe compiles
-exactly those source lines, read from the reference tree where they lie, inside
-small harness kernels of this repository:
+PyRoFFI (absent).  The sampling, tree-balance, nearest-neighbour, extend,
+dynamic-domain, waypoint and connect arithmetic of its planner does not depend
+on either, so this recipe compiles exactly those source lines, read from the
+reference tree where they lie, inside small harness kernels of this repository:
 
+  cuda-rrtc/CUDA/prrtc_planner.cu:46-83     dynamic-domain radius shrink / grow (CAS loops)
   cuda-rrtc/CUDA/prrtc_planner.cu:144-157   halton_next_runtime
   cuda-rrtc/CUDA/prrtc_planner.cu:748-758   per-block prime shuffle
   cuda-rrtc/CUDA/prrtc_planner.cu:784-788   Halton sample
+  cuda-rrtc/CUDA/prrtc_planner.cu:792-823   tree-side balance (all four modes)
   cuda-rrtc/CUDA/prrtc_planner.cu:842-862   nearest-neighbour scan + block reduction
   cuda-rrtc/CUDA/prrtc_planner.cu:864-878   extend / dynamic-domain skip
   cuda-rrtc/CUDA/prrtc_planner.cu:899-904   edge waypoint interpolation
@@ -21,11 +23,15 @@ nvcc compiles them with the reference's flags (-O3, default FMA contraction), so
 the harness outputs are the reference's own device results.  Output goes only to
 oracle/_ref/ (git-ignored).  Nothing is copied into the repository.
 
+The reference tree is found at --reference, else $PRRTC_REFERENCE_DIR, else
+/root/reference.
+
 Usage: python oracle/ref/build_ref.py [--reference DIR]
 """
 from __future__ import annotations
 
 import argparse
+import os
 import shutil
 import subprocess
 import sys
@@ -35,10 +41,12 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE.parent / "_ref"
 OUT = OUT_DIR / "libprrtc_ref.so"
-DEFAULT_REF = Path("/root/reference")
+DEFAULT_REF = Path(os.environ.get("PRRTC_REFERENCE_DIR", "/root/reference"))
 
 # (file, first line, last line, text that must appear on the first line)
 FRAGMENTS = {
+    "radius": ("cuda-rrtc/CUDA/prrtc_planner.cu", 46, 83, "prrtc_radius_shrink_atomic"),
+    "balance": ("cuda-rrtc/CUDA/prrtc_planner.cu", 792, 823, "const int size_a"),
     "halton": ("cuda-rrtc/CUDA/prrtc_planner.cu", 144, 157, "halton_next_runtime"),
     "primes": ("cuda-rrtc/CUDA/prrtc_planner.cu", 748, 758, "int primes[16]"),
     "sample": ("cuda-rrtc/CUDA/prrtc_planner.cu", 784, 788, "for (int d = 0; d < dim; ++d)"),
@@ -66,7 +74,43 @@ HARNESS = r'''
 #include <math.h>
 #include "prrtc_helpers.cuh"
 
+@radius@
+
 @halton@
+
+// Dynamic-domain updates: update i is op[i] (0 shrink, 1 grow) on radii[idx[i]];
+// one thread per update (contending CAS loops) or, with sequential, one thread
+// applying them in order.
+__global__ void h_radius(float* radii, const int* idx, const int* op, int n, float dd_alpha, float dd_radius,
+                         float dd_min_radius, int sequential) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k0 = sequential ? 0 : i, k1 = sequential ? n : i + 1;
+    if (sequential && i != 0) return;
+    for (int k = k0; k < k1 && k < n; ++k) {
+        if (op[k] == 0) prrtc_radius_shrink_atomic(radii, idx[k], dd_alpha, dd_radius, dd_min_radius);
+        else prrtc_radius_grow_atomic(radii, idx[k], dd_alpha);
+    }
+}
+
+// Tree-side balance of explorer bid = blockIdx.x of gridDim.x for n cases:
+// sizes [n][2], local_iters [n], vamp_in / tree_out / vamp_out [n][gridDim.x].
+__global__ void h_balance(int* sizes, const int* local_iters, const int* vamp_in, int n, int balance_mode,
+                          float tree_ratio, int* tree_out, int* vamp_out) {
+    if (threadIdx.x != 0) return;
+    const int bid = blockIdx.x;
+    for (int c = 0; c < n; ++c) {
+        int* tree_sizes = sizes + 2 * c;
+        const int local_iter = local_iters[c];
+        int vamp_tree_id = vamp_in[c * gridDim.x + bid];
+        int t_tree_id_sh = -1, o_tree_id_sh = -1;
+        {
+@balance@
+        }
+        tree_out[c * gridDim.x + bid] = t_tree_id_sh;
+        vamp_out[c * gridDim.x + bid] = vamp_tree_id;
+        (void)o_tree_id_sh;
+    }
+}
 
 __global__ void h_samples(int explorer, int n, int dim, const float* min_vals, const float* max_vals, float* out) {
     if (threadIdx.x != 0) return;
@@ -152,6 +196,19 @@ __global__ void h_connect(const float* o_cfgs, int max_nodes, int dim, const flo
 @extend_kernel@
 
 extern "C" {
+int ref_radius(float* radii, const int* idx, const int* op, int n, float alpha, float r0, float rmin, int sequential,
+               void* s) {
+    if (n <= 0) return 0;
+    h_radius<<<sequential ? 1 : (n + 127) / 128, sequential ? 32 : 128, 0, (cudaStream_t)s>>>(
+        radii, idx, op, n, alpha, r0, rmin, sequential);
+    return (int)cudaGetLastError();
+}
+int ref_balance(int* sizes, const int* local_iters, const int* vamp_in, int n, int nblocks, int mode, float ratio,
+                int* tree_out, int* vamp_out, void* s) {
+    if (n <= 0 || nblocks < 1) return -1;
+    h_balance<<<nblocks, 32, 0, (cudaStream_t)s>>>(sizes, local_iters, vamp_in, n, mode, ratio, tree_out, vamp_out);
+    return (int)cudaGetLastError();
+}
 int ref_halton_samples(int explorer, int n, int dim, const float* lo, const float* hi, float* out, void* s) {
     h_samples<<<1, 32, 0, (cudaStream_t)s>>>(explorer, n, dim, lo, hi, out);
     return (int)cudaGetLastError();

@@ -102,7 +102,9 @@ EXPORTS = (
     "prrtc_b200_check_edges_workspace_size", "prrtc_b200_check_edges",
     "prrtc_b200_fk", "prrtc_b200_halton", "prrtc_b200_extract_paths",
     "prrtc_b200_smooth_workspace_size", "prrtc_b200_smooth_cost_grad",
-    "prrtc_b200_fp32_probe",
+    "prrtc_b200_smooth_batch_workspace_size", "prrtc_b200_smooth_cost_grad_batch",
+    "prrtc_b200_choose_tree", "prrtc_b200_radius_update",
+    "prrtc_b200_fp32_probe", "prrtc_b200_fp32x2_probe",
     "prrtc_b200_error_string", "prrtc_b200_last_cuda_error", "prrtc_b200_version",
 )
 
@@ -126,7 +128,12 @@ _SIGS = {
     "prrtc_b200_extract_paths": (C.c_int, [I32, I32, I32, P, P, P, P, P, P, I32, P, P, P, P]),
     "prrtc_b200_smooth_workspace_size": (C.c_size_t, [P, P]),
     "prrtc_b200_smooth_cost_grad": (C.c_int, [P, P, I32, P, I32, I32, F32, F32, F32, P, P, P, C.c_size_t, P]),
+    "prrtc_b200_smooth_batch_workspace_size": (C.c_size_t, [P]),
+    "prrtc_b200_smooth_cost_grad_batch": (C.c_int, [P, I32, P, I32, F32, F32, F32, P, P, P, C.c_size_t, P]),
+    "prrtc_b200_choose_tree": (C.c_int, [I32, I32, P, P, P, I32, F32, P, P, P]),
+    "prrtc_b200_radius_update": (C.c_int, [P, P, P, I32, F32, F32, F32, I32, P, P]),
     "prrtc_b200_fp32_probe": (C.c_int, [I32, I32, I32, P, P]),
+    "prrtc_b200_fp32x2_probe": (C.c_int, [I32, I32, I32, P, P]),
     "prrtc_b200_error_string": (C.c_char_p, [C.c_int]),
     "prrtc_b200_last_cuda_error": (C.c_int, []),
     "prrtc_b200_version": (C.c_int, []),

@@ -2,8 +2,7 @@
 
 For one capacity bucket, times a plan of the bucket's problems for each
 candidate (explorers per problem = samples per iteration, threads per explorer
--- 32 meaning one explorer per warp, four per CTA --, waypoints per
-shared-memory chunk, CTAs per SM) by solved plans per second: the median of three launches
+(one explorer per CTA), waypoints per shared-memory chunk, CTAs per SM) by solved plans per second: the median of three launches
 per candidate, then a second round between the three best (six more launches
 each, taken in turn) decides; L2 is flushed before every timed launch.  Results
 are cached per (device, bucket, problem count, shape) in
@@ -18,7 +17,7 @@ from pathlib import Path
 import torch
 
 SAMPLES = (1, 2, 4, 8, 16)
-THREADS = (64, 128, 256)  # 32 (one explorer per warp) stays available but lost on every bucket measured
+THREADS = (64, 128, 256)  # 32 stays available (a one-warp CTA) but is slower on every bucket measured
 CHUNKS = (8, 16, 32)
 CTAS_PER_SM = (0, 2)  # 0: as many as fit; 2: two, with the rest of shared memory given to L1
 CANDIDATES = tuple((e, t, c, r) for r in CTAS_PER_SM for t in THREADS for c in CHUNKS for e in SAMPLES)

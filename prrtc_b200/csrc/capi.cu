@@ -2,6 +2,7 @@
 // Argument validation mirrors the reference's Python checks (cuda-rrtc/jax/
 // prrtc.py:353-381: power-of-two granularity <= 64, step_size > 0) plus the
 // compile-time limits of its kernels (CONFIG_DIM_MAX 16, PRRTC_MAX_JOINTS 64).
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -136,7 +137,6 @@ static void fill_launch(PlanLaunch& L, const prrtc_outputs_t* out, const prrtc_a
     L.dd_alpha = a->dd_alpha; L.dd_radius = a->dd_radius; L.dd_min_radius = a->dd_min_radius;
     L.edge_res = tu.edge_res; L.threads = tu.threads; L.cw = tu.cw; L.resident = tu.resident;
     L.stats = tu.stats;
-    L.warp_explorers = tu.threads == 32;
     L.pc = pc_view(tu.cloud);
     L.tail_join = tu.tail_join;
     L.wait_polls = tu.wait_polls;
@@ -436,6 +436,27 @@ int prrtc_b200_halton(int32_t explorer, int32_t n, int32_t dim, const float* lo,
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 
+int prrtc_b200_choose_tree(int32_t mode, int32_t n, const int32_t* sizes, const int32_t* local_iter,
+                           const int32_t* vamp_in, int32_t nblocks, float tree_ratio, int32_t* tree_out,
+                           int32_t* vamp_out, void* stream) {
+    if (n == 0) return PRRTC_B200_OK;
+    if (n < 0 || mode < 0 || nblocks < 1 || nblocks > (1 << 24) || !sizes || !local_iter || !vamp_in || !tree_out ||
+        !vamp_out)
+        return PRRTC_B200_EARG;
+    cudaError_t e = launch_choose_tree(mode, n, sizes, local_iter, vamp_in, nblocks, tree_ratio, tree_out, vamp_out,
+                                       static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
+int prrtc_b200_radius_update(float* radii, const int32_t* idx, const int32_t* op, int32_t n, float alpha, float r0,
+                             float rmin, int32_t sequential, int32_t* err, void* stream) {
+    if (n == 0) return PRRTC_B200_OK;
+    if (n < 0 || !radii || !idx || !op) return PRRTC_B200_EARG;
+    cudaError_t e = launch_radius_update(radii, idx, op, n, alpha, r0, rmin, sequential, err,
+                                         static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
 int prrtc_b200_extract_paths(int32_t batch, int32_t dim, int32_t max_nodes, const float* ta, const float* tb,
                              const int32_t* pa, const int32_t* pb, const int32_t* conn, const int32_t* solved,
                              int32_t max_len, float* paths, int32_t* lengths, float* costs, void* stream) {
@@ -474,8 +495,36 @@ int prrtc_b200_smooth_cost_grad(const prrtc_robot_t* robot, const prrtc_world_t*
     unsigned char* blob = static_cast<unsigned char*>(ws);
     cudaError_t e = launch_pack(s, 1, blob, stride, st);
     if (e != cudaSuccess) return cuda_fail(e);
-    e = launch_smooth(blob, world->self_pairs, s.J, s.S, dim, waypoints, n_paths, n_waypoints, margin, beta, w_len,
-                      cost, grad, nullptr, st);
+    e = launch_smooth(blob, 0, world->self_pairs, 0, s.J, s.S, dim, waypoints, n_paths, n_waypoints, margin, beta,
+                      w_len, cost, grad, st);
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
+size_t prrtc_b200_smooth_batch_workspace_size(const prrtc_batch_inputs_t* in) {
+    if (!in || in->batch < 1) return 0;
+    return (size_t)in->batch * blob_stride(make_batch_pack(in, 1, 0, 0.0f));
+}
+
+int prrtc_b200_smooth_cost_grad_batch(const prrtc_batch_inputs_t* in, int32_t dim, const float* waypoints,
+                                      int32_t n_waypoints, float margin, float beta, float w_len, float* cost,
+                                      float* grad, void* ws, size_t ws_bytes, void* stream) {
+    if (!in) return PRRTC_B200_EARG;
+    if (in->batch == 0) return PRRTC_B200_OK;
+    if (in->batch < 0 || !waypoints || !cost || n_waypoints < 1 || !(beta > 0.0f)) return PRRTC_B200_EARG;
+    if (dim < 1 || dim > PRRTC_B200_DIM_MAX) return PRRTC_B200_EUNSUPPORTED;
+    if (in->robot.n_joints < 1 || in->robot.n_joints > PRRTC_B200_MAX_JOINTS) return PRRTC_B200_EUNSUPPORTED;
+    int rc = check_robot(in->robot);
+    if (rc) return rc;
+    const PackSrc s = make_batch_pack(in, dim, 0, 0.0f);  // flat model, as the single-scene form
+    const size_t stride = blob_stride(s);
+    if (!ws || !aligned(ws, 256) || ws_bytes < (size_t)in->batch * stride) return PRRTC_B200_EWORKSPACE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char* blobs = static_cast<unsigned char*>(ws);
+    cudaError_t e = launch_pack(s, in->batch, blobs, stride, st);
+    if (e != cudaSuccess) return cuda_fail(e);
+    const size_t pstride = in->self_pairs_count ? (size_t)std::max(0, in->max_self_pairs) : 0;
+    e = launch_smooth(blobs, stride, in->self_pairs, pstride, s.J, s.S, dim, waypoints, in->batch, n_waypoints,
+                      margin, beta, w_len, cost, grad, st);
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 
@@ -493,21 +542,48 @@ int prrtc_b200_smooth_cost_grad(const prrtc_robot_t* robot, const prrtc_world_t*
 static __device__ __align__(256) unsigned char g_noalloc_scene[PRRTC_B200_NOALLOC_SCENE_MAX];
 
 static std::mutex g_noalloc_mutex;
-static unsigned char* g_noalloc_ptr[256];  // device address of g_noalloc_scene, per device ordinal
+// Device address of g_noalloc_scene per device ordinal, with the CUDA context it
+// belongs to: the address is valid only in that context.
+static unsigned char* g_noalloc_ptr[256];
+static CUcontext g_noalloc_ctx[256];
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+// The driver's cuCtxGetCurrent, looked up through the runtime (no link against
+// libcuda): the context a device address belongs to.
+static CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    return fn;
+}
 
 // Host code cannot use g_noalloc_scene's name as a device address: resolve it
-// once per device, with that device current.
+// with the device current, once per device and context.  A call made in a
+// context other than the one of the cached address (another driver context made
+// current, or the primary context re-created after cudaDeviceReset) resolves it
+// again.
 static int noalloc_scene_ptr(unsigned char** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e);
     if (dev < 0 || dev >= 256) return PRRTC_B200_EUNSUPPORTED;
+    const CtxGetCurrentFn get_ctx = ctx_get_current();
+    CUcontext ctx = nullptr;
+    if (get_ctx && get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
         void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scene);
+        e = cudaGetSymbolAddress(&p, g_noalloc_scene);  // makes the device's primary context current if none is
         if (e != cudaSuccess) return cuda_fail(e);
+        if (get_ctx && get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
         g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = g_noalloc_ptr[dev];
     return PRRTC_B200_OK;
@@ -538,6 +614,12 @@ int prrtc_b200_check_configs_noalloc(const prrtc_robot_t* robot, const prrtc_wor
 int prrtc_b200_fp32_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink, void* stream) {
     if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || !sink) return PRRTC_B200_EARG;
     cudaError_t e = launch_fp32_probe(blocks, threads, iters, sink, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
+int prrtc_b200_fp32x2_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink, void* stream) {
+    if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1 || !sink) return PRRTC_B200_EARG;
+    cudaError_t e = launch_fp32x2_probe(blocks, threads, iters, sink, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 

@@ -71,7 +71,6 @@ struct PlanLaunch {
     // tuning
     int threads, cw, resident;
     int persistent;
-    int warp_explorers;                // persistent form with 32 threads: one explorer per warp (4 per CTA)
     int tail_join;                     // persistent form: idle CTAs join running problems as extra explorers
     int wait_polls;                    // polls of the scene-staging wait before it gives up (0: default, <0: none)
     int ctas_per_sm;                   // persistent form: > 0 caps CTAs per SM and sizes the shared-memory carve-out
@@ -113,14 +112,21 @@ struct FkTables {
 cudaError_t launch_fk(const FkTables& t, int dim, const float* configs, int n, float* frames, cudaStream_t st);
 cudaError_t launch_halton(int explorer, int n, int dim, const float* lo, const float* hi, float* out,
                           cudaStream_t st);
+cudaError_t launch_choose_tree(int mode, int n, const int32_t* sizes, const int32_t* local_iter,
+                               const int32_t* vamp_in, int nblocks, float tree_ratio, int32_t* tree_out,
+                               int32_t* vamp_out, cudaStream_t st);
+cudaError_t launch_radius_update(float* radii, const int32_t* idx, const int32_t* op, int n, float alpha, float r0,
+                                 float rmin, int sequential, int32_t* err, cudaStream_t st);
 
 // smooth.cu
-cudaError_t launch_smooth(const unsigned char* blob, const int32_t* pairs, int J, int S, int dim,
-                          const float* wp, int P, int W, float margin, float beta, float w_len, float* cost,
-                          float* grad, float* scratch, cudaStream_t st);
-size_t smooth_scratch_bytes(int J, int S, int P, int W);
+// Path p uses the scene at blob + p * blob_stride and the self pairs at
+// pairs + 2 * p * pairs_stride (strides 0: one scene for every path).
+cudaError_t launch_smooth(const unsigned char* blob, size_t blob_stride, const int32_t* pairs, size_t pairs_stride,
+                          int J, int S, int dim, const float* wp, int P, int W, float margin, float beta, float w_len,
+                          float* cost, float* grad, cudaStream_t st);
 
 cudaError_t launch_fp32_probe(int blocks, int threads, int iters, float* sink, cudaStream_t st);
+cudaError_t launch_fp32x2_probe(int blocks, int threads, int iters, float* sink, cudaStream_t st);
 
 int device_sm_count();
 size_t device_max_smem();

@@ -125,6 +125,44 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
         const float* c = &wh[i * 6];
         o_wh[i] = make_float4(c[0], c[1], c[2], -(c[0] * c[3] + c[1] * c[4] + c[2] * c[5]));
     }
+    // packed copies for the pair-wise tests (layout at pk_bytes in prrtc_device.cuh),
+    // the same values as the plain records, each duplicated into a pair
+    float4* pk_s = reinterpret_cast<float4*>(blob + L.o_pk);
+    for (int i = tid; i < 2 * ((Ns + 1) / 2); i += T) {
+        const int p = i >> 1, half = i & 1;
+        float4 O = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float B = INFINITY;  // pad: never a hit
+        if (i < Ns) {
+            const float x = ws[i * 4], y = ws[i * 4 + 1], z = ws[i * 4 + 2], r = ws[i * 4 + 3];
+            O = make_float4(-2.0f * x, -2.0f * y, -2.0f * z, -2.0f * r);
+            B = fmaf(x, x, fmaf(y, y, fmaf(z, z, -r * r)));
+        }
+        pk_s[5 * p + 2 * half] = make_float4(O.x, O.x, O.y, O.y);
+        pk_s[5 * p + 2 * half + 1] = make_float4(O.z, O.z, O.w, O.w);
+        reinterpret_cast<float2*>(&pk_s[5 * p + 4])[half] = make_float2(B, B);
+    }
+    float4* pk_c = reinterpret_cast<float4*>(blob + L.o_pk + pk_sphere_bytes(Ns));
+    for (int i = tid; i < Nc; i += T) {
+        const float4 p1r = o_wc[3 * i], dp = o_wc[3 * i + 1], d = o_wc[3 * i + 2];
+        pk_c[6 * i] = make_float4(dp.x, dp.x, dp.y, dp.y);
+        pk_c[6 * i + 1] = make_float4(dp.z, dp.z, dp.w, dp.w);
+        pk_c[6 * i + 2] = make_float4(p1r.x, p1r.x, p1r.y, p1r.y);
+        pk_c[6 * i + 3] = make_float4(p1r.z, p1r.z, p1r.w, p1r.w);
+        pk_c[6 * i + 4] = make_float4(-d.x, -d.x, -d.y, -d.y);
+        pk_c[6 * i + 5] = make_float4(-d.z, -d.z, -p1r.w, -p1r.w);
+    }
+    float4* pk_b = pk_c + 6 * Nc;
+    for (int i = tid; i < Nb; i += T) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float4 a = o_wb[4 * i + k];
+            pk_b[8 * i + 2 * k] = make_float4(a.x, a.x, a.y, a.y);
+            pk_b[8 * i + 2 * k + 1] = make_float4(a.z, a.z, a.w, a.w);
+        }
+        const float4 h = o_wb[4 * i + 3];
+        pk_b[8 * i + 6] = make_float4(h.x, h.x, h.y, h.y);
+        pk_b[8 * i + 7] = make_float4(h.z, h.z, 0.0f, 0.0f);
+    }
     int2* cp = reinterpret_cast<int2*>(blob + L.o_cpair);
     for (int q = tid; q < Q; q += T) cp[q] = make_int2(s.cpairs[2 * q], s.cpairs[2 * q + 1]);
     // dense-block detection: coarse pair q's range is the row-major product of
@@ -215,7 +253,7 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
         hd.o_joint = L.o_joint; hd.o_sph = L.o_sph; hd.o_sfr = L.o_sfr; hd.o_grp = L.o_grp;
         hd.o_sch = L.o_sch; hd.o_ws = L.o_ws; hd.o_wc = L.o_wc; hd.o_wb = L.o_wb;
         hd.o_wh = L.o_wh; hd.o_item = L.o_item; hd.o_cpair = L.o_cpair; hd.used_bytes = L.bytes;
-        hd.P = P; hd.cap_bytes = cap; hd.error = overflow ? 1 : 0; hd.pad0 = 0;
+        hd.P = P; hd.cap_bytes = cap; hd.error = overflow ? kBlobItemOverflow : 0; hd.o_pk = L.o_pk;
         *h = hd;
     }
 }
@@ -228,66 +266,6 @@ cudaError_t launch_pack(const PackSrc& s, int batch, unsigned char* blobs, size_
 }
 
 // ============================================================================ helpers
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* mbar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_addr(mbar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-
-constexpr int kWaitLimit = 1 << 22;
-
-// Bulk-copy `bytes` (multiple of 16; both addresses 16-byte aligned) from global
-// memory into shared memory and wait for completion with a bounded spin of
-// `first_limit` polls.  All threads call it; returns false (uniformly) if the
-// wait ran out, after setting *err and giving the copy a second bounded wait to
-// land.
-__device__ bool stage_blob(unsigned char* dst, const unsigned char* src, int bytes, uint64_t* mbar,
-                           uint32_t& phase, int* err, int first_limit) {
-    __syncthreads();  // previous readers of dst are done
-    if (threadIdx.x == 0) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        uint64_t state;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                     : "=l"(state)
-                     : "r"(smem_addr(mbar)), "r"(bytes)
-                     : "memory");
-        (void)state;
-        for (int off = 0; off < bytes; off += 16384) {
-            const int n = min(16384, bytes - off);
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    smem_addr(dst + off)),
-                "l"(src + off), "r"(n), "r"(smem_addr(mbar))
-                : "memory");
-        }
-    }
-    bool ok = false;
-    for (int i = 0; i < first_limit && !ok; ++i) ok = mbar_try_wait(mbar, phase);
-    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
-    if (!all_ok) {
-        // the wait ran out: report it, then let the copy land (bounded) before
-        // the CTA stops using -- or leaves -- its shared memory
-        if (threadIdx.x == 0 && err) atomicExch(err, 1);
-        for (int i = 0; i < kWaitLimit && !ok; ++i) ok = mbar_try_wait(mbar, phase);
-        __syncthreads();
-    }
-    phase ^= 1u;
-    return all_ok;
-}
 
 // ============================================================================ nearest neighbour
 
@@ -347,26 +325,21 @@ __device__ void group_nearest(const G& grp, const float* __restrict__ tree, int 
         const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
         if (od < best || (od == best && oi < bi)) { best = od; bi = oi; }
     }
-    if constexpr (G::kWarp) {
-        if (tid == 0) { red_d[0] = best; red_i[0] = bi; }
-        grp.sync();
-    } else {
-        const int warp = tid >> 5, lane = tid & 31, nwarp = (T + 31) >> 5;
-        if (lane == 0) { red_d[warp] = best; red_i[warp] = bi; }
-        __syncthreads();
-        if (warp == 0) {
-            best = lane < nwarp ? red_d[lane] : INFINITY;
-            bi = lane < nwarp ? red_i[lane] : INT_MAX;
+    const int warp = tid >> 5, lane = tid & 31, nwarp = (T + 31) >> 5;
+    if (lane == 0) { red_d[warp] = best; red_i[warp] = bi; }
+    grp.sync();
+    if (warp == 0) {
+        best = lane < nwarp ? red_d[lane] : INFINITY;
+        bi = lane < nwarp ? red_i[lane] : INT_MAX;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const float od = __shfl_xor_sync(0xffffffffu, best, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                if (od < best || (od == best && oi < bi)) { best = od; bi = oi; }
-            }
-            if (lane == 0) { red_d[0] = best; red_i[0] = bi; }
+        for (int off = 16; off > 0; off >>= 1) {
+            const float od = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (od < best || (od == best && oi < bi)) { best = od; bi = oi; }
         }
-        __syncthreads();
+        if (lane == 0) { red_d[0] = best; red_i[0] = bi; }
     }
+    grp.sync();
 }
 
 // ============================================================================ explorer
@@ -428,28 +401,6 @@ __device__ int tail_join_pick(const PlanLaunch& L, int* e_out) {
         if (ld_volatile(&L.solved[bb]) == 0) return bb;
     }
     return -1;
-}
-
-// Tree side (prrtc_planner.cu:790-824); nblocks = explorers of this problem.
-__device__ int choose_tree(int mode, int local_iter, int bid, int nblocks, int size_a, int size_b, float thr,
-                           int& vamp) {
-    const int total = size_a + size_b;
-    if (mode == 0 || local_iter == 1) return (bid < (nblocks / 2)) ? 0 : 1;
-    if (mode == 1) {
-        const int diff = size_a >= size_b ? size_a - size_b : size_b - size_a;
-        const float ratio = total > 0 ? __fdiv_rn((float)size_a, (float)total) : 0.5f;
-        if (diff < (int)(1.5f * (float)nblocks)) return (bid < (int)((float)nblocks * (1.0f - ratio))) ? 0 : 1;
-        return ratio < thr ? 0 : 1;
-    }
-    if (mode == 2) {
-        const int o_id = 1 - vamp;
-        const int t_sz = vamp == 0 ? size_a : size_b;
-        const int o_sz = o_id == 0 ? size_a : size_b;
-        const float r = t_sz > 0 ? fabsf(__fdiv_rn((float)(t_sz - o_sz), (float)t_sz)) : 0.0f;
-        if (r < thr) vamp = 1 - vamp;
-        return vamp;
-    }
-    return size_a <= size_b ? 0 : 1;
 }
 
 // Edge [base, base+delta] at waypoints t = (k+1)/G (prrtc_planner.cu:899-903).
@@ -561,7 +512,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
         grp.sync();
         if (X.skip) continue;
         if (group_edge_collides(grp, sc, B, X.base, X.delta, X.G1, L.cw, par)) {
-            if (tid == 0 && L.dd) radius_shrink(P.radii[t], X.nn, L.dd_alpha, L.dd_radius, L.dd_min_radius);
+            if (tid == 0 && L.dd) radius_shrink(P.radii[t], X.nn, L.dd_alpha, L.dd_radius, L.dd_min_radius, &L.queue[1]);
             continue;
         }
         // insert (prrtc_planner.cu:925-947)
@@ -572,7 +523,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
                 X.new_idx = -1;
             } else {
                 P.par[t][idx] = X.nn;
-                if (L.dd) radius_grow(P.radii[t], X.nn, L.dd_alpha);
+                if (L.dd) radius_grow(P.radii[t], X.nn, L.dd_alpha, &L.queue[1]);
                 X.new_idx = idx;
             }
         }
@@ -716,7 +667,9 @@ __global__ void __launch_bounds__(256) explore_kernel(PlanLaunch L) {
         if (b != cur) {
             if (staged) {
                 const int bytes = reinterpret_cast<const BlobHeader*>(gblob)->used_bytes;
-                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1], L.wait_polls == 0 ? kWaitLimit : max(L.wait_polls, 0))) break;
+                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1], 1,
+                                L.wait_polls == 0 ? kWaitLimit : max(L.wait_polls, 0)))
+                    break;
                 sc = scene_view(blob_sm);
             } else {
                 sc = scene_view(gblob);
@@ -731,82 +684,56 @@ __global__ void __launch_bounds__(256) explore_kernel(PlanLaunch L) {
     }
 }
 
-// Persistent batched form with one explorer per warp: a CTA pops a group of
-// kWarpsPerCta explorer slots of one problem, stages that problem's scene once,
-// and each warp runs one explorer with warp-level synchronisation only.
-constexpr int kWarpsPerCta = 4;
+// Slot initialisation (the reference's memsets and FLT_MAX fill,
+// prrtc_planner.cu:1192-1202, 85-95): slots [0, cap_b) of problem b's rows --
+// two trees of dim rows, two parent rows, two radius rows -- become
+// 0xFFFFFFFF in the trees and parents (a NaN tree slot, skipped by the
+// nearest-neighbour scan until written; parent -1) and FLT_MAX in the radii
+// (unset).  Only the problem's own
+// capacity is written; words [cap_b, N) of its rows are never read by the
+// planner and keep whatever they held.  A CTA writes 16 KB chunks of one row
+// (uint4 stores when every row starts 16-byte aligned, N % 4 == 0); blockIdx.y
+// strides over problems, blockIdx.x over a problem's (row, chunk) items.
+constexpr int kFillChunk = 4096;  // 32-bit words per fill item
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32) explore_warps_kernel(PlanLaunch L) {
-    extern __shared__ __align__(128) unsigned char dsm[];
-    __shared__ ExplorerSmem Xs[kWarpsPerCta];
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ int s_group;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const bool staged = L.blob_cap > 0;
-    unsigned char* blob_sm = dsm;
-    const int ccb = cc_smem_bytes(L.J, L.S, L.K, L.Q, L.cw);
-    CcBufs B = cc_bufs(dsm + (staged ? L.blob_cap : 0) + warp * ccb, L.J, L.S, L.K, L.Q, L.cw);
-    B.stats = L.stats;
-    ExplorerSmem& X = Xs[warp];
-    if (tid == 0) mbar_init(&mbar);
-    __syncthreads();
-    uint32_t phase = 0;
-    int cur = -1;
-    Scene sc;
-    const int gpp = (L.E + kWarpsPerCta - 1) / kWarpsPerCta;  // slot groups per problem
-    const int total = L.B * gpp;
-    __shared__ int s_join_b, s_join_e;
-    while (true) {
-        if (tid == 0) {
-            int g = atomicAdd(&L.queue[0], 1);
-            while (g < total) {  // skip problems that already terminated
-                const int pi = g / gpp;
-                const int bb = L.order ? L.order[pi] : pi;
-                if (ld_volatile(&L.solved[bb]) == 0) break;
-                g = atomicAdd(&L.queue[0], 1);
-            }
-            s_group = g;
-            s_join_b = -1;
-            if (g >= total && L.tail_join) {
-                int e0;
-                s_join_b = tail_join_pick(L, &e0);
-                s_join_e = L.E + (e0 - L.E) * kWarpsPerCta;  // four distinct extra explorers
-            }
-        }
-        __syncthreads();
-        const int g = s_group;
-        int b, e;
-        if (g < total) {
-            const int pi = g / gpp;
-            b = L.order ? L.order[pi] : pi;
-            e = (g - pi * gpp) * kWarpsPerCta + warp;
-        } else {
-            if (s_join_b < 0) break;
-            b = s_join_b;
-            e = s_join_e + warp;
-        }
-        const unsigned char* gblob = L.blobs + (size_t)b * L.blob_stride;
-        if (b != cur) {
-            if (staged) {
-                const int bytes = reinterpret_cast<const BlobHeader*>(gblob)->used_bytes;
-                if (!stage_blob(blob_sm, gblob, min(bytes, L.blob_cap), &mbar, phase, &L.queue[1], L.wait_polls == 0 ? kWaitLimit : max(L.wait_polls, 0))) break;
-                sc = scene_view(blob_sm);
+__device__ __forceinline__ uint32_t* fill_row(const PlanLaunch& L, int b, int r) {
+    const size_t N = (size_t)L.N;
+    if (r < L.dim) return reinterpret_cast<uint32_t*>(L.tree_a) + ((size_t)b * L.dim + r) * N;
+    r -= L.dim;
+    if (r < L.dim) return reinterpret_cast<uint32_t*>(L.tree_b) + ((size_t)b * L.dim + r) * N;
+    r -= L.dim;
+    if (r == 0) return reinterpret_cast<uint32_t*>(L.par_a) + (size_t)b * N;
+    if (r == 1) return reinterpret_cast<uint32_t*>(L.par_b) + (size_t)b * N;
+    return reinterpret_cast<uint32_t*>(L.radii) + ((size_t)b * 2 + (r - 2)) * N;
+}
+
+__global__ void __launch_bounds__(256) fill_kernel(PlanLaunch L) {
+    const int rows = 2 * L.dim + 4;
+    const bool vec = (L.N & 3) == 0;
+    for (int b = blockIdx.y; b < L.B; b += gridDim.y) {
+        const int cap = L.caps ? max(1, min(L.caps[b], L.N)) : L.N;
+        const int chunks = (cap + kFillChunk - 1) / kFillChunk;
+        for (int it = blockIdx.x; it < rows * chunks; it += gridDim.x) {
+            const int r = it / chunks, c0 = (it - r * chunks) * kFillChunk;
+            const int c1 = min(cap, c0 + kFillChunk);
+            uint32_t* row = fill_row(L, b, r);
+            const uint32_t w = r >= 2 * L.dim + 2 ? 0x7f7fffffu : ~0u;  // FLT_MAX radii, else all ones
+            if (vec) {
+                // c0 is a multiple of 4; the last vector may pass cap but stays
+                // inside the row (N % 4 == 0), in words nobody reads
+                uint4* v = reinterpret_cast<uint4*>(row + c0);
+                const int n4 = (c1 - c0 + 3) >> 2;
+                for (int k = threadIdx.x; k < n4; k += blockDim.x) v[k] = make_uint4(w, w, w, w);
             } else {
-                sc = scene_view(gblob);
+                for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) row[k] = w;
             }
-            sc.pairs = reinterpret_cast<const int2*>(L.pairs) + (size_t)b * L.pairs_stride;
-            sc.pc = L.pc;
-            cur = b;
         }
-        const Prob P = prob_ptrs(L, b);
-        if (tid == 0) atomicCAS(&P.ts[0], 0ull, globaltimer());
-        if (e < L.E || g >= total) run_explorer(WarpGroup{}, L, P, sc, B, X, e);
-        __syncthreads();  // every warp done with this problem before the next pop
     }
 }
 
 // Roots and counters (prrtc_planner.cu:97-125, 1204-1237).  Tree slots,
-// parents and radii were byte-filled with 0xFF (NaN / -1 / unset) before.
+// parents and radii of [0, cap_b) were set (NaN / -1 / FLT_MAX) by fill_kernel
+// before.
 __global__ void init_kernel(PlanLaunch L, int stamp_start) {
     const int b = blockIdx.x, tid = threadIdx.x;
     if (b >= L.B) return;
@@ -882,31 +809,26 @@ size_t device_max_smem() {
 
 cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
     cudaError_t e;
-    const size_t tn = (size_t)L.B * L.dim * L.N * sizeof(float);
-    if ((e = cudaMemsetAsync(L.tree_a, 0xFF, tn, st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(L.tree_b, 0xFF, tn, st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(L.par_a, 0xFF, (size_t)L.B * L.N * sizeof(int32_t), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(L.par_b, 0xFF, (size_t)L.B * L.N * sizeof(int32_t), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(L.radii, 0xFF, (size_t)L.B * 2 * L.N * sizeof(float), st)) != cudaSuccess) return e;
+    {
+        // enough fill CTAs for about four per SM in total, at least 16 per problem
+        const int gy = std::min(L.B, 65535);
+        const int gx = std::max(16, (4 * device_sm_count() + gy - 1) / gy);
+        fill_kernel<<<dim3(gx, gy), 256, 0, st>>>(L);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     init_kernel<<<L.B, 128, 0, st>>>(L, L.persistent ? 0 : 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
-    const size_t ccb = (size_t)cc_smem_bytes(L.J, L.S, L.K, L.Q, L.cw);
+    const size_t cc = (size_t)cc_smem_bytes(L.J, L.S, L.K, L.Q, L.cw);
     const size_t max_smem = device_max_smem();
-    // one explorer per warp needs four checker buffers; fall back to one
-    // explorer per (single-warp) CTA when they do not fit
-    const bool warps = L.persistent && L.warp_explorers &&
-                       (ccb + sizeof(ExplorerSmem)) * kWarpsPerCta + 64 <= max_smem;
-    const size_t cc = ccb * (warps ? kWarpsPerCta : 1);
-    const size_t static_smem = sizeof(ExplorerSmem) * (warps ? kWarpsPerCta : 1) + 64;
+    const size_t static_smem = sizeof(ExplorerSmem) + 64;
     size_t dyn = cc + (size_t)L.blob_cap;
     if (dyn + static_smem > max_smem) {  // scene too large to stage: read it from global memory
         L.blob_cap = 0;
         dyn = cc;
     }
-    auto kern = warps ? explore_warps_kernel : explore_kernel;
-    const int threads = warps ? kWarpsPerCta * 32 : L.threads;
-    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(explore_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) !=
+        cudaSuccess)
         return e;
     // ctas_per_sm > 0: the smallest shared-memory carve-out that holds that many
     // CTAs, so the rest of the SM's unified L1 / shared memory is L1 (the
@@ -920,26 +842,28 @@ cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
         cudaGetDevice(&dev);
         if ((e = cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess ||
             (e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess ||
-            (e = cudaFuncGetAttributes(&fa, kern)) != cudaSuccess)
+            (e = cudaFuncGetAttributes(&fa, explore_kernel)) != cudaSuccess)
             return e;
         const size_t need = (size_t)L.ctas_per_sm * (dyn + fa.sharedSizeBytes + (size_t)reserved);
         carve = sm_smem > 0 ? (int)std::min<size_t>(100, (100 * need + sm_smem - 1) / (size_t)sm_smem) : -1;
     }
-    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, carve)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(explore_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carve)) !=
+        cudaSuccess)
         return e;
     if (L.persistent) {
         int per_sm = 0;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, dyn)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, explore_kernel, L.threads, dyn)) !=
+            cudaSuccess)
+            return e;
         per_sm = std::max(per_sm, 1);
         if (L.ctas_per_sm > 0) per_sm = std::min(per_sm, L.ctas_per_sm);
         long long grid = (long long)per_sm * device_sm_count();
         if (L.resident > 0) grid = std::min<long long>(grid, L.resident);
-        const long long work = warps ? (long long)L.B * ((L.E + kWarpsPerCta - 1) / kWarpsPerCta) : (long long)L.B * L.E;
         // no more CTAs than explorer slots: with several batches in flight (one per
         // capacity bucket) a full-GPU grid per launch measured slower, its CTAs
         // piling extra explorers onto a few problems
-        grid = std::min<long long>(grid, work);
-        kern<<<(unsigned)std::max<long long>(grid, 1), threads, dyn, st>>>(L);
+        grid = std::min<long long>(grid, (long long)L.B * L.E);
+        explore_kernel<<<(unsigned)std::max<long long>(grid, 1), L.threads, dyn, st>>>(L);
     } else {
         explore_kernel<<<dim3(L.E, L.B), L.threads, dyn, st>>>(L);
     }

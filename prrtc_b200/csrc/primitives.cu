@@ -286,13 +286,11 @@ cudaError_t launch_iteration(float* ta, float* tb, int32_t* pa, int32_t* pb, int
 
 // ============================================================================ batched collision check
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
 // Persistent over chunks of CW configurations; the scene is bulk-copied into
-// shared memory once per CTA (bounded wait; on timeout the CTA reads the scene
-// from global memory instead).
+// shared memory once per CTA.  The wait is bounded: when it runs out, the CTA
+// sets bit kBlobStagingTimeout of the blob header's `error` word (global
+// memory), lets the copy land (second bounded wait) and reads the scene from
+// global memory instead -- the verdicts are the same either way.
 #ifndef PRRTC_CHECK_CW
 #define PRRTC_CHECK_CW 32       // configurations per CTA pass of the batched checker
 #endif
@@ -313,37 +311,12 @@ __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const
     Scene sc;
     if (staged) {
         const int bytes = min(reinterpret_cast<const BlobHeader*>(gblob)->used_bytes, blob_cap);
-        if (tid == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
+        if (tid == 0) mbar_init(&mbar);
         __syncthreads();
-        if (tid == 0) {
-            uint64_t state;
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                         : "=l"(state)
-                         : "r"(smem_u32(&mbar)), "r"(bytes)
-                         : "memory");
-            (void)state;
-            for (int off = 0; off < bytes; off += 16384) {
-                const int m = min(16384, bytes - off);
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        smem_u32(dsm + off)),
-                    "l"(gblob + off), "r"(m), "r"(smem_u32(&mbar))
-                    : "memory");
-            }
-        }
-        uint32_t done = 0;
-        for (int i = 0; i < (1 << 22) && !done; ++i) {
-            asm volatile(
-                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
-                : "=r"(done)
-                : "r"(smem_u32(&mbar))
-                : "memory");
-        }
-        const int all = __syncthreads_and(done ? 1 : 0);
-        sc = scene_view(all ? dsm : gblob);
+        uint32_t phase = 0;
+        int* err = reinterpret_cast<int*>(const_cast<unsigned char*>(gblob) + offsetof(BlobHeader, error));
+        const bool ok = stage_blob(dsm, gblob, bytes, &mbar, phase, err, kBlobStagingTimeout, kWaitLimit);
+        sc = scene_view(ok ? dsm : gblob);
     } else {
         sc = scene_view(gblob);
     }
@@ -439,6 +412,59 @@ cudaError_t launch_halton(int explorer, int n, int dim, const float* lo, const f
     return cudaGetLastError();
 }
 
+// ============================================================================ planner rules
+
+// Tree-side choice of the planner (choose_tree) for n cases at once: explorer
+// bid = blockIdx.x of nblocks = gridDim.x, case c with tree sizes sizes[2c],
+// sizes[2c+1], the explorer's iteration count local_iter[c] and its mode-2 side
+// vamp_in[c * nblocks + bid]; writes the chosen tree and the updated side.
+__global__ void choose_tree_kernel(int mode, int n, const int32_t* sizes, const int32_t* local_iter,
+                                   const int32_t* vamp_in, float tree_ratio, int32_t* tree_out, int32_t* vamp_out) {
+    const int bid = blockIdx.x, nblocks = gridDim.x;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        int vamp = vamp_in[(size_t)c * nblocks + bid];
+        const int t = choose_tree(mode, local_iter[c], bid, nblocks, sizes[2 * c], sizes[2 * c + 1], tree_ratio, vamp);
+        tree_out[(size_t)c * nblocks + bid] = t;
+        vamp_out[(size_t)c * nblocks + bid] = vamp;
+    }
+}
+
+cudaError_t launch_choose_tree(int mode, int n, const int32_t* sizes, const int32_t* local_iter,
+                               const int32_t* vamp_in, int nblocks, float tree_ratio, int32_t* tree_out,
+                               int32_t* vamp_out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    choose_tree_kernel<<<nblocks, 128, 0, st>>>(mode, n, sizes, local_iter, vamp_in, tree_ratio, tree_out, vamp_out);
+    return cudaGetLastError();
+}
+
+// Dynamic-domain radius updates of the planner (radius_shrink / radius_grow):
+// update i is op[i] (0 shrink, 1 grow) on radii[idx[i]].  Concurrent: one
+// thread per update, so updates of one index contend on its CAS loop;
+// sequential: one thread applies them in order.
+__global__ void radius_update_kernel(float* radii, const int32_t* idx, const int32_t* op, int n, float alpha,
+                                     float r0, float rmin, int sequential, int32_t* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sequential) {
+        if (i != 0) return;
+        for (int k = 0; k < n; ++k) {
+            if (op[k] == 0) radius_shrink(radii, idx[k], alpha, r0, rmin, err);
+            else radius_grow(radii, idx[k], alpha, err);
+        }
+        return;
+    }
+    if (i >= n) return;
+    if (op[i] == 0) radius_shrink(radii, idx[i], alpha, r0, rmin, err);
+    else radius_grow(radii, idx[i], alpha, err);
+}
+
+cudaError_t launch_radius_update(float* radii, const int32_t* idx, const int32_t* op, int n, float alpha, float r0,
+                                 float rmin, int sequential, int32_t* err, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    radius_update_kernel<<<sequential ? 1 : (n + 127) / 128, sequential ? 32 : 128, 0, st>>>(
+        radii, idx, op, n, alpha, r0, rmin, sequential, err);
+    return cudaGetLastError();
+}
+
 // ============================================================================ FP32 probe
 
 // 8 independent FFMA chains per thread: the FP32 pipe stays busy without
@@ -460,6 +486,44 @@ __global__ void fp32_probe_kernel(int iters, float* sink) {
 
 cudaError_t launch_fp32_probe(int blocks, int threads, int iters, float* sink, cudaStream_t st) {
     fp32_probe_kernel<<<blocks, threads, 0, st>>>(iters, sink);
+    return cudaGetLastError();
+}
+
+// The same with packed FP32 (fma.rn.f32x2, sm_100): 8 independent chains of two
+// lanes each per thread, 2 * 2 * 8 * 16 * iters flops per thread.  Measures
+// whether one packed instruction delivers two FP32 FMAs per lane per issue
+// slot, i.e. which FP32 peak a kernel built from packed FMAs runs against.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__global__ void fp32x2_probe_kernel(int iters, float* sink) {
+    const float b = threadIdx.x * 1e-7f;
+    unsigned long long a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = pack2(b + (2 * k) * 1e-7f, b + (2 * k + 1) * 1e-7f);
+    const unsigned long long m = pack2(0.999999f, 0.999999f), c = pack2(1e-7f, 1e-7f);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) asm volatile("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(a[k]) : "l"(m), "l"(c));
+        }
+    }
+    float r = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        float lo, hi;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a[k]));
+        r += lo + hi;
+    }
+    if (r == 12345.0f) sink[blockIdx.x] = r;  // never true; keeps the chains live
+}
+
+cudaError_t launch_fp32x2_probe(int blocks, int threads, int iters, float* sink, cudaStream_t st) {
+    fp32x2_probe_kernel<<<blocks, threads, 0, st>>>(iters, sink);
     return cudaGetLastError();
 }
 

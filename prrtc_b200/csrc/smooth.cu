@@ -53,6 +53,8 @@ __device__ __forceinline__ float log1p_unit(float e) {
 struct SmoothArgs {
     const unsigned char* blob;
     const int2* pairs;
+    size_t blob_stride;   // bytes between the scenes of consecutive paths (0: one scene for every path)
+    size_t pairs_stride;  // int2 between the self-pair lists of consecutive paths (0: shared list)
     int J, S, dim;
     const float* wp;
     int P, W;
@@ -90,7 +92,8 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
     const int c = blockIdx.x * WARPS + warp;
     if (c >= a.P * a.W) return;
     const int p = c / a.W, w = c - p * a.W;
-    const Scene sc = scene_view(a.blob);
+    const Scene sc = scene_view(a.blob + (size_t)p * a.blob_stride);
+    const int2* pairs = a.pairs + (size_t)p * a.pairs_stride;
     const BlobHeader& h = *sc.h;
     const int J = a.J, S = a.S, dim = a.dim;
     float* base = smf + (size_t)warp * smooth_warp_floats(J, S);
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
     __syncwarp();
     // 2b. self pairs (explicit list): shared-memory atomics into both spheres
     for (int k = lane; k < h.P; k += 32) {
-        const int2 pr = __ldg(&a.pairs[k]);
+        const int2 pr = __ldg(&pairs[k]);
         if (pr.x < 0 || pr.y < 0 || pr.x >= S || pr.y >= S) continue;
         if (sc.sfr[pr.x] < 0 || sc.sfr[pr.y] < 0) continue;
         const float4 ci = ctr[pr.x], cj = ctr[pr.y];
@@ -283,11 +286,9 @@ __global__ void __launch_bounds__(WARPS * 32) smooth_kernel(SmoothArgs a) {
     if (lane == 0) atomicAdd(&a.cost[p], cost);
 }
 
-size_t smooth_scratch_bytes(int, int, int, int) { return 0; }
-
-cudaError_t launch_smooth(const unsigned char* blob, const int32_t* pairs, int J, int S, int dim, const float* wp,
-                          int P, int W, float margin, float beta, float w_len, float* cost, float* grad, float*,
-                          cudaStream_t st) {
+cudaError_t launch_smooth(const unsigned char* blob, size_t blob_stride, const int32_t* pairs, size_t pairs_stride,
+                          int J, int S, int dim, const float* wp, int P, int W, float margin, float beta, float w_len,
+                          float* cost, float* grad, cudaStream_t st) {
     if (P <= 0 || W <= 0) return cudaSuccess;
     constexpr int WARPS = 4;
     cudaError_t e = cudaMemsetAsync(cost, 0, (size_t)P * sizeof(float), st);
@@ -298,7 +299,8 @@ cudaError_t launch_smooth(const unsigned char* blob, const int32_t* pairs, int J
                                       (int)smem)) != cudaSuccess)
             return e;
     }
-    SmoothArgs a{blob, reinterpret_cast<const int2*>(pairs), J, S, dim, wp, P, W, margin, beta, w_len, cost, grad};
+    SmoothArgs a{blob, reinterpret_cast<const int2*>(pairs), blob_stride, pairs_stride, J, S, dim, wp, P, W,
+                 margin, beta, w_len, cost, grad};
     const long long n = (long long)P * W;
     smooth_kernel<WARPS><<<(unsigned)((n + WARPS - 1) / WARPS), WARPS * 32, smem, st>>>(a);
     return cudaGetLastError();

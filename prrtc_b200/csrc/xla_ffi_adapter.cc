@@ -7,14 +7,20 @@
 // adds -DPRRTC_WITH_XLA_FFI and jaxlib's include directory).  The binding order,
 // names and dtypes are the reference's interface contract
 // (cuda-rrtc/CUDA/prrtc_planner.cu:1946-2117, prrtc_nearest_neighbor.cu:132-141,
-// prrtc_extend.cu:129-140).  Unlike the reference handlers these never block the
-// host and allocate only when their per-device workspace must grow.
+// prrtc_extend.cu:129-140).  Unlike the reference handlers (cudaMalloc / cudaFree
+// of their scratch and a blocking event sync per call) these never block the host
+// and never call the CUDA allocator: each call's workspace, sized by the
+// library's *_workspace_size query, comes from XLA's own scratch allocator
+// (ffi::ScratchAllocator, bound as a context argument).  XLA releases that
+// memory when the handler returns; its device allocator hands it out again only
+// to work ordered after this call on the same compute stream, which is where the
+// kernels run.
 #if defined(PRRTC_WITH_XLA_FFI)
 
 #include <cuda_runtime.h>
 
-#include <mutex>
-#include <vector>
+#include <optional>
+#include <string>
 
 #include "../../include/prrtc_b200.h"
 #include "xla/ffi/api/ffi.h"
@@ -23,30 +29,16 @@ namespace ffi = xla::ffi;
 
 namespace {
 
-// Per-device workspace that only grows (allocation happens outside any steady
-// state: the first call of a given size).
-struct Pool {
-    std::mutex m;
-    std::vector<void*> ptr;
-    std::vector<size_t> bytes;
-    void* get(size_t need, cudaError_t* err) {
-        int dev = 0;
-        *err = cudaGetDevice(&dev);
-        if (*err != cudaSuccess) return nullptr;
-        std::lock_guard<std::mutex> lock(m);
-        if ((int)ptr.size() <= dev) { ptr.resize(dev + 1, nullptr); bytes.resize(dev + 1, 0); }
-        if (bytes[dev] < need) {
-            if (ptr[dev]) cudaFree(ptr[dev]);
-            ptr[dev] = nullptr;
-            bytes[dev] = 0;
-            *err = cudaMalloc(&ptr[dev], need);
-            if (*err != cudaSuccess) return nullptr;
-            bytes[dev] = need;
-        }
-        return ptr[dev];
-    }
-};
-Pool g_pool;
+// 256-byte aligned workspace of `need` bytes from XLA's scratch allocator.
+void* scratch_bytes(ffi::ScratchAllocator& scratch, size_t need) {
+    std::optional<void*> p = scratch.Allocate(need > 0 ? need : 256, 256);
+    return p.has_value() ? *p : nullptr;
+}
+
+ffi::Error no_scratch(size_t need) {
+    return ffi::Error(ffi::ErrorCode::kResourceExhausted,
+                      "prrtc_b200: XLA scratch allocation of " + std::to_string(need) + " bytes failed");
+}
 
 template <typename B>
 int rows(const B& b) { return b.dimensions().size() == 0 ? 0 : static_cast<int>(b.dimensions()[0]); }
@@ -92,7 +84,7 @@ prrtc_attrs_t attrs_of(int max_iterations, float step_size, int num_new_samples,
     return a;
 }
 
-ffi::Error PlannerImpl(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi, F32 tw, F32 ptf, S32 par, S32 act,
+ffi::Error PlannerImpl(cudaStream_t stream, ffi::ScratchAllocator scratch, F32 start, F32 goals, F32 lo, F32 hi, F32 tw, F32 ptf, S32 par, S32 act,
                        F32 mm, F32 mo, S32 mact, S32 topo, S32 sli, F32 sloc, F32 srad, F32 ws, F32 wc, F32 wb, F32 wh,
                        S32 sp, S32 cli, F32 cloc, F32 crad, S32 foff, S32 cpairs, S32 cranges, RF32 ta, RF32 tb,
                        RS32 pa, RS32 pb, RS32 sizes, RS32 completed, RS32 iters, RS32 conn, RS32 solved, RF32 ktime,
@@ -118,9 +110,8 @@ ffi::Error PlannerImpl(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi
                                      dynamic_domain, dd_alpha, dd_radius, dd_min_radius, dim, max_nodes, granularity,
                                      collision_mode, collision_margin);
     const size_t need = prrtc_b200_plan_workspace_size(&in, &a, nullptr);
-    cudaError_t e;
-    void* w = g_pool.get(need, &e);
-    if (!w) return ffi::Error(ffi::ErrorCode::kInternal, cudaGetErrorString(e));
+    void* w = scratch_bytes(scratch, need);
+    if (!w) return no_scratch(need);
     return status(prrtc_b200_plan(&in, &out, &a, nullptr, w, need, stream));
 }
 
@@ -134,7 +125,7 @@ prrtc_outputs_t outputs_of(RF32 ta, RF32 tb, RS32 pa, RS32 pb, RS32 sizes, RS32 
 // Batched planners (prrtc_planner.cu:1404-1944).  ctx: worlds are [B, max_n,
 // feat] with per-problem counts ("prrtc_planner_batch_ctx"); otherwise one
 // shared world ("prrtc_planner_batch", count pointers NULL).
-ffi::Error run_batch(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi, const prrtc_robot_t& robot,
+ffi::Error run_batch(cudaStream_t stream, ffi::ScratchAllocator& scratch, F32 start, F32 goals, F32 lo, F32 hi, const prrtc_robot_t& robot,
                      F32 ws, F32 wc, F32 wb, F32 wh, S32 sp, const int32_t* cws, const int32_t* cwc,
                      const int32_t* cwb, const int32_t* cwh, const int32_t* csp, bool batched,
                      const prrtc_outputs_t& out, const prrtc_attrs_t& a) {
@@ -160,13 +151,12 @@ ffi::Error run_batch(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi, 
     in.self_pairs = sp.typed_data(); in.max_self_pairs = max_n(sp); in.self_pairs_count = csp;
     in.problem_order = nullptr;
     const size_t need = prrtc_b200_plan_batch_workspace_size(&in, &a, nullptr);
-    cudaError_t e;
-    void* w = g_pool.get(need, &e);
-    if (!w) return ffi::Error(ffi::ErrorCode::kInternal, cudaGetErrorString(e));
+    void* w = scratch_bytes(scratch, need);
+    if (!w) return no_scratch(need);
     return status(prrtc_b200_plan_batch(&in, &out, &a, nullptr, w, need, stream));
 }
 
-ffi::Error BatchCtxImpl(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi, F32 tw, F32 ptf, S32 par,
+ffi::Error BatchCtxImpl(cudaStream_t stream, ffi::ScratchAllocator scratch, F32 start, F32 goals, F32 lo, F32 hi, F32 tw, F32 ptf, S32 par,
                         S32 act, F32 mm, F32 mo, S32 mact, S32 topo, S32 sli, F32 sloc, F32 srad, F32 ws, F32 wc,
                         F32 wb, F32 wh, S32 sp, S32 nws, S32 nwc, S32 nwb, S32 nwh, S32 nsp, S32 cli, F32 cloc,
                         F32 crad, S32 foff, S32 cpairs, S32 cranges, RF32 ta, RF32 tb, RS32 pa, RS32 pb,
@@ -179,12 +169,12 @@ ffi::Error BatchCtxImpl(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 h
     const prrtc_attrs_t a = attrs_of(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio,
                                      dynamic_domain, dd_alpha, dd_radius, dd_min_radius, dim, max_nodes, granularity,
                                      collision_mode, collision_margin);
-    return run_batch(stream, start, goals, lo, hi, robot, ws, wc, wb, wh, sp, nws.typed_data(), nwc.typed_data(),
+    return run_batch(stream, scratch, start, goals, lo, hi, robot, ws, wc, wb, wh, sp, nws.typed_data(), nwc.typed_data(),
                      nwb.typed_data(), nwh.typed_data(), nsp.typed_data(), true,
                      outputs_of(ta, tb, pa, pb, sizes, completed, iters, conn, solved, ktime), a);
 }
 
-ffi::Error BatchImpl(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi, F32 tw, F32 ptf, S32 par, S32 act,
+ffi::Error BatchImpl(cudaStream_t stream, ffi::ScratchAllocator scratch, F32 start, F32 goals, F32 lo, F32 hi, F32 tw, F32 ptf, S32 par, S32 act,
                      F32 mm, F32 mo, S32 mact, S32 topo, S32 sli, F32 sloc, F32 srad, F32 ws, F32 wc, F32 wb,
                      F32 wh, S32 sp, S32 cli, F32 cloc, F32 crad, S32 foff, S32 cpairs, S32 cranges, RF32 ta,
                      RF32 tb, RS32 pa, RS32 pb, RS32 sizes, RS32 completed, RS32 iters, RS32 conn, RS32 solved,
@@ -196,21 +186,20 @@ ffi::Error BatchImpl(cudaStream_t stream, F32 start, F32 goals, F32 lo, F32 hi, 
     const prrtc_attrs_t a = attrs_of(max_iterations, step_size, num_new_samples, balance_mode, tree_ratio,
                                      dynamic_domain, dd_alpha, dd_radius, dd_min_radius, dim, max_nodes, granularity,
                                      collision_mode, collision_margin);
-    return run_batch(stream, start, goals, lo, hi, robot, ws, wc, wb, wh, sp, nullptr, nullptr, nullptr, nullptr,
+    return run_batch(stream, scratch, start, goals, lo, hi, robot, ws, wc, wb, wh, sp, nullptr, nullptr, nullptr, nullptr,
                      nullptr, false, outputs_of(ta, tb, pa, pb, sizes, completed, iters, conn, solved, ktime), a);
 }
 
 // prrtc_nearest_neighbor.cu:80-141; the tree size is read on the device (no host sync).
-ffi::Error NearestNeighborImpl(cudaStream_t stream, F32 tree, F32 queries, S32 tree_size, RS32 indices, RF32 dists) {
+ffi::Error NearestNeighborImpl(cudaStream_t stream, ffi::ScratchAllocator scratch, F32 tree, F32 queries, S32 tree_size, RS32 indices, RF32 dists) {
     const auto td = tree.dimensions();
     if (td.size() != 2) return ffi::Error(ffi::ErrorCode::kInvalidArgument, "tree_configs must be [dim, max_nodes]");
     const int dim = static_cast<int>(td[0]), max_nodes = static_cast<int>(td[1]);
     const int batch = rows(queries);
     if (batch == 0) return ffi::Error::Success();
     const size_t need = prrtc_b200_nearest_neighbor_workspace_size(batch);
-    cudaError_t e;
-    void* w = g_pool.get(need, &e);
-    if (!w) return ffi::Error(ffi::ErrorCode::kInternal, cudaGetErrorString(e));
+    void* w = scratch_bytes(scratch, need);
+    if (!w) return no_scratch(need);
     return status(prrtc_b200_nearest_neighbor(tree.typed_data(), dim, max_nodes, tree_size.typed_data(),
                                               queries.typed_data(), batch, indices->typed_data(),
                                               dists->typed_data(), w, need, stream));
@@ -250,6 +239,7 @@ ffi::Error IterationImpl(cudaStream_t stream, F32 ta, F32 tb, S32 pa, S32 pb, F3
 #define PRRTC_PLANNER_BINDING                                                                          \
     ffi::Ffi::Bind()                                                                                   \
         .Ctx<ffi::PlatformStream<cudaStream_t>>()                                                      \
+        .Ctx<ffi::ScratchAllocator>()                                                                  \
         .Arg<F32>().Arg<F32>().Arg<F32>().Arg<F32>()                /* start, goals, min, max */       \
         .Arg<F32>().Arg<F32>().Arg<S32>().Arg<S32>()                /* twists, parent_tf, parent, act */ \
         .Arg<F32>().Arg<F32>().Arg<S32>().Arg<S32>()                /* mimic mul/off/act, topo_inv */  \
@@ -288,6 +278,7 @@ XLA_FFI_DEFINE_HANDLER_SYMBOL(PrrtcPlannerFfi, PlannerImpl, PRRTC_PLANNER_BINDIN
 XLA_FFI_DEFINE_HANDLER_SYMBOL(PrrtcPlannerBatchCtxFfi, BatchCtxImpl,
                               ffi::Ffi::Bind()
                                   .Ctx<ffi::PlatformStream<cudaStream_t>>()
+                                  .Ctx<ffi::ScratchAllocator>()
                                   .Arg<F32>().Arg<F32>().Arg<F32>().Arg<F32>()  /* start, goals, min, max */
                                   PRRTC_ROBOT_ARGS
                                   .Arg<F32>().Arg<F32>().Arg<F32>().Arg<F32>().Arg<S32>()  /* batched worlds */
@@ -298,6 +289,7 @@ XLA_FFI_DEFINE_HANDLER_SYMBOL(PrrtcPlannerBatchCtxFfi, BatchCtxImpl,
 XLA_FFI_DEFINE_HANDLER_SYMBOL(PrrtcPlannerBatchFfi, BatchImpl,
                               ffi::Ffi::Bind()
                                   .Ctx<ffi::PlatformStream<cudaStream_t>>()
+                                  .Ctx<ffi::ScratchAllocator>()
                                   .Arg<F32>().Arg<F32>().Arg<F32>().Arg<F32>()  /* start, goals, min, max */
                                   PRRTC_ROBOT_ARGS
                                   .Arg<F32>().Arg<F32>().Arg<F32>().Arg<F32>().Arg<S32>()  /* shared world */
@@ -307,6 +299,7 @@ XLA_FFI_DEFINE_HANDLER_SYMBOL(PrrtcPlannerBatchFfi, BatchImpl,
 XLA_FFI_DEFINE_HANDLER_SYMBOL(PrrtcNearestNeighborFfi, NearestNeighborImpl,
                               ffi::Ffi::Bind()
                                   .Ctx<ffi::PlatformStream<cudaStream_t>>()
+                                  .Ctx<ffi::ScratchAllocator>()
                                   .Arg<F32>().Arg<F32>().Arg<S32>()
                                   .Ret<S32>().Ret<F32>());
 

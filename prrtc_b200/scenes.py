@@ -15,7 +15,8 @@ benchmark workloads:
 * worlds        -- ``spheres_world`` (16 spheres in [-.8,.8]^2 x [0,1.2]),
                    ``tabletop_world`` (floor halfspace, table + 3-5 shelf slabs +
                    clutter boxes, capsules, spheres), ``uneven_world`` (4-128
-                   spheres, 0-32 boxes), ``large_world`` (256 spheres, 64 boxes,
+                   spheres, 0-32 boxes), ``dense_world`` (the same counts at the
+                   16-sphere scene's density, larger boxes), ``large_world`` (256 spheres, 64 boxes,
                    floor).
 
 Start and goal configurations are rejection-sampled collision free by a caller
@@ -190,7 +191,7 @@ def dual_arm(seed: int = 0) -> RobotModel:
 BASE_KEEPOUT = 0.3  # obstacles never intersect the column |xy| < 0.3 m around the arm base
 
 
-def _centres(rng, n, lo, hi, clearance):
+def _centres(rng, n, lo, hi, clearance, keepout=BASE_KEEPOUT):
     """n points uniform in [lo, hi] whose xy distance to a base column exceeds keep-out + clearance."""
     bases = _BASES
     out = np.zeros((0, 3))
@@ -198,7 +199,7 @@ def _centres(rng, n, lo, hi, clearance):
         c = rng.uniform(lo, hi, size=(max(4 * n, 16), 3))
         ok = np.ones(c.shape[0], bool)
         for bx, by in bases:
-            ok &= np.hypot(c[:, 0] - bx, c[:, 1] - by) > BASE_KEEPOUT + clearance
+            ok &= np.hypot(c[:, 0] - bx, c[:, 1] - by) > keepout + clearance
         out = np.concatenate([out, c[ok]], 0)
     return out[:n]
 
@@ -274,6 +275,29 @@ def uneven_world(rng) -> dict:
     nb = int(rng.integers(0, 33))
     if nb:
         w["world_boxes"] = _random_boxes(rng, nb, UNEVEN_LO, UNEVEN_HI)
+    return w
+
+
+DENSE_LO, DENSE_HI = (-0.8, -0.8, 0.0), (0.8, 0.8, 1.2)
+DENSE_KEEPOUT = 0.15  # just clear of the arm's first link: any obstacle there blocks every configuration
+
+
+def dense_world(rng) -> dict:
+    """The uneven counts (4-128 spheres, 0-32 boxes) at the density of the
+    16-sphere scene: spheres (r 0.05-0.15) and boxes (half extents 0.02-0.3,
+    random yaw) in [-0.8,0.8]^2 x [0,1.2], clear only of a 0.15 m column around
+    the base.  About 2-25% of the configuration space is free, and some start /
+    goal pairs lie in different free components (unsolvable problems)."""
+    w = empty_world()
+    n = int(rng.integers(4, 129))
+    r = rng.uniform(0.05, 0.15, size=(n, 1))
+    c = _centres(rng, n, DENSE_LO, DENSE_HI, 0.15, DENSE_KEEPOUT)
+    w["world_spheres"] = np.concatenate([c, r], 1).astype(np.float32)
+    nb = int(rng.integers(0, 33))
+    if nb:
+        cs = _centres(rng, nb, DENSE_LO, DENSE_HI, float(np.sqrt(2.0)) * 0.3, DENSE_KEEPOUT)
+        boxes = [_yaw_box(ci, rng.uniform(-np.pi, np.pi), rng.uniform(0.02, 0.3, 3)) for ci in cs]
+        w["world_boxes"] = np.asarray(boxes, np.float32).reshape(-1, 15)
     return w
 
 
@@ -354,7 +378,7 @@ BUCKETS = (4096, 16384, 65536)
 
 
 def make_problem(kind: str, seed: int, checker: Checker, robot: RobotModel | None = None) -> Problem:
-    """Problem ``seed`` of workload ``kind``: spheres16 | tabletop | uneven | large | pointcloud."""
+    """Problem ``seed`` of workload ``kind``: spheres16 | tabletop | uneven | dense | large | pointcloud."""
     rng = np.random.default_rng(seed)
     if kind == "large":
         robot = robot or dual_arm(0)
@@ -364,8 +388,8 @@ def make_problem(kind: str, seed: int, checker: Checker, robot: RobotModel | Non
         world, n_goals, max_nodes = spheres_world(rng, 16), 1, 65536
     elif kind == "tabletop":
         world, n_goals, max_nodes = tabletop_world(rng), 4, 65536
-    elif kind == "uneven":
-        world = uneven_world(rng)
+    elif kind in ("uneven", "dense"):
+        world = uneven_world(rng) if kind == "uneven" else dense_world(rng)
         n_goals = int(rng.integers(1, 9))
         n_obs = world["world_spheres"].shape[0] + world["world_boxes"].shape[0]
         max_nodes = BUCKETS[0] if n_obs < 48 else (BUCKETS[1] if n_obs < 112 else BUCKETS[2])

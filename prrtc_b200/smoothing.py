@@ -92,17 +92,20 @@ def densify(paths: torch.Tensor, resolution: float) -> tuple[torch.Tensor, torch
     """Points every <= `resolution` (joint-space L2) along each polyline [P, W, dim];
     returns configs [M, dim] and the path index of each point."""
     P, W, dim = paths.shape
+    dev = paths.device
     d = torch.linalg.norm(paths[:, 1:] - paths[:, :-1], dim=-1)           # [P, W-1]
     n = torch.clamp(torch.ceil(d / resolution), min=1).to(torch.int64)    # [P, W-1]
-    n_cpu = n.cpu().numpy()
-    pts, owner = [], []
-    for p in range(P):
-        for w in range(W - 1):
-            k = int(n_cpu[p, w])
-            t = torch.arange(0, k + 1 if w == W - 2 else k, device=paths.device, dtype=paths.dtype) / k
-            pts.append(paths[p, w][None] + t[:, None] * (paths[p, w + 1] - paths[p, w])[None])
-            owner.append(torch.full((t.shape[0],), p, device=paths.device, dtype=torch.int64))
-    return torch.cat(pts, 0), torch.cat(owner, 0)
+    # segment (p, w) gives points t = k / n for k < n, the last one also t = 1
+    cnt = n.clone()
+    cnt[:, -1] += 1
+    cnt = cnt.reshape(-1)
+    seg = torch.repeat_interleave(torch.arange(cnt.numel(), device=dev), cnt)
+    first = torch.cumsum(cnt, 0) - cnt
+    k = torch.arange(seg.numel(), device=dev) - first[seg]
+    t = k.to(paths.dtype) / n.reshape(-1)[seg].to(paths.dtype)
+    p, w = seg // (W - 1), seg % (W - 1)
+    a, b = paths[p, w], paths[p, w + 1]
+    return a + t[:, None] * (b - a), p
 
 
 def smooth_paths(paths: list, collision_context: dict, lower, upper, *, waypoints: int = 64, steps: int = 50,
@@ -137,3 +140,103 @@ def smooth_paths(paths: list, collision_context: dict, lower, upper, *, waypoint
     accepted = bad == 0
     out = torch.where(accepted[:, None, None], x, init)
     return out, accepted, c0, c1
+
+
+class BatchSmoothContext:
+    """Robot tables plus one world per path, resident on the device, for the
+    batched adjoint (prrtc_b200_smooth_cost_grad_batch): path p is costed
+    against collision_contexts[p]'s world and self pairs."""
+
+    def __init__(self, collision_contexts, dim: int, margin: float = 0.02, beta: float = 50.0, w_len: float = 1.0,
+                 device=None):
+        from .prrtc import _pack_worlds
+
+        self.lib = _lib.load()
+        self.device = cuda_device(device)
+        self.dim = int(dim)
+        self.margin, self.beta, self.w_len = float(margin), float(beta), float(w_len)
+        ctxs = list(collision_contexts)
+        B = self.B = len(ctxs)
+        self.robot_ctx = DeviceContext(ctxs[0], self.device, world_keys=False)
+        packed, counts = _pack_worlds(ctxs, B)
+        self.t = {}
+        bi = _lib.BatchInputs()
+        bi.batch = B
+        bi.robot = self.robot_ctx.robot()
+        for key in ("world_spheres", "world_capsules", "world_boxes", "world_halfspaces", "self_pairs"):
+            tab = torch.from_numpy(np.ascontiguousarray(packed[key])).to(self.device)
+            cnt = torch.from_numpy(np.ascontiguousarray(counts[key], dtype=np.int32)).to(self.device)
+            self.t[key], self.t[key + "_count"] = tab, cnt
+            setattr(bi, key, tab.data_ptr() if tab.numel() else None)
+            setattr(bi, "max_" + key, int(tab.shape[1]))
+            setattr(bi, key + "_count", cnt.data_ptr())
+        self.bi = bi
+        self.ws = workspace(self.lib.prrtc_b200_smooth_batch_workspace_size(C.byref(bi)), self.device)
+
+    def cost_grad(self, waypoints: torch.Tensor, need_grad: bool = True):
+        wp = waypoints.detach().to(self.device, torch.float32).contiguous()
+        P, W, dim = wp.shape
+        if P != self.B:
+            raise ValueError(f"expected {self.B} paths (one per world), got {P}")
+        cost = torch.empty((P,), dtype=torch.float32, device=self.device)
+        grad = torch.empty_like(wp) if need_grad else None
+        _lib.check(self.lib.prrtc_b200_smooth_cost_grad_batch(C.byref(self.bi), dim, ptr(wp), W, self.margin,
+                                                              self.beta, self.w_len, ptr(cost), ptr(grad),
+                                                              self.ws.data_ptr(), self.ws.numel(), stream_handle()),
+                   "prrtc_b200_smooth_cost_grad_batch")
+        return cost, grad
+
+
+def projected_steps(sctx, init: torch.Tensor, lower, upper, steps: int, lr: float) -> torch.Tensor:
+    """`steps` projected gradient steps of the adjoint cost from `init` [P, W, dim]:
+    endpoints fixed, joint limits enforced, step length lr per path (the
+    gradient normalised per path)."""
+    P, W, dim = init.shape
+    lo = as_tensor(lower, torch.float32, init.device).reshape(1, 1, dim)
+    hi = as_tensor(upper, torch.float32, init.device).reshape(1, 1, dim)
+    x = init.clone()
+    mask = torch.ones_like(x)
+    mask[:, 0] = 0.0
+    mask[:, -1] = 0.0
+    for _ in range(steps):
+        _, g = sctx.cost_grad(x)
+        gn = torch.linalg.norm((g * mask).reshape(P, -1), dim=1).clamp_min(1e-12)
+        x = torch.minimum(torch.maximum(x - lr * (g * mask) / gn[:, None, None], lo), hi)
+    return x
+
+
+def smooth_paths_batch(paths: list, collision_contexts: list, lower, upper, *, waypoints: int = 64,
+                       steps: int = 50, lr: float = 0.05, margin: float = 0.02, beta: float = 50.0,
+                       w_len: float = 1.0, resolution: float = 0.01, device=None):
+    """smooth_paths for the paths of a batch plan, path p in its own world
+    collision_contexts[p]: one batched adjoint launch per step for all paths,
+    then exact re-validation of each smoothed path at `resolution` against its
+    world; a path that fails reverts to its input.
+
+    Returns (smoothed [P, waypoints, dim], accepted [P] bool, cost before [P],
+    cost after [P])."""
+    dev = cuda_device(device)
+    dim = int(np.asarray(paths[0]).shape[1])
+    init = torch.from_numpy(np.stack([resample_path(p, waypoints) for p in paths])).to(dev)
+    sctx = BatchSmoothContext(collision_contexts, dim, margin, beta, w_len, dev)
+    c0, _ = sctx.cost_grad(init, need_grad=False)
+    x = projected_steps(sctx, init, lower, upper, steps, lr)
+    c1, _ = sctx.cost_grad(x, need_grad=False)
+    accepted = revalidate_batch(x, collision_contexts, resolution, dev)
+    out = torch.where(accepted[:, None, None], x, init)
+    return out, accepted, c0, c1
+
+
+def revalidate_batch(paths: torch.Tensor, collision_contexts: list, resolution: float, device) -> torch.Tensor:
+    """Exact binary re-validation of path p [W, dim] of `paths` at `resolution`
+    against collision_contexts[p]; returns accepted [P] bool."""
+    pts, owner = densify(paths, resolution)
+    owner_np = owner.cpu().numpy()
+    bounds = np.searchsorted(owner_np, np.arange(paths.shape[0] + 1))
+    accepted = torch.ones((paths.shape[0],), dtype=torch.bool, device=device)
+    for p, ctx in enumerate(collision_contexts):
+        seg = pts[bounds[p]:bounds[p + 1]]
+        if seg.shape[0]:
+            v = CollisionChecker(ctx, paths.shape[2], "binary", 0.0, device).check(seg)
+            accepted[p] = v.max() == 0
+    return accepted

@@ -5,11 +5,18 @@ Explorers race on the GPU, so trees differ run to run (the reference says the
 same: verify_coarse_equivalence.py:3-8); what must agree are the distributions.
 The batched planner runs with exactly num_new_samples explorers per problem
 (tail_explorers=False), as the reference and the oracle do.
-Criteria, at 95%: the Wilson intervals of the two success rates overlap, and the
-bootstrap intervals of the two median path costs overlap.  Every GPU path is
-re-validated with the float64 binary checker at 0.01 rad.
 
-PRRTC_DIST_PROBLEMS sets the problem count (default 1000, tabletop workload).
+Workload: the dense uneven scenes (4-128 spheres and 0-32 boxes of half extents
+up to 0.3 m in [-0.8,0.8]^2 x [0,1.2]), where 2-25% of configuration space is
+free and some start / goal pairs are disconnected, with a tight iteration
+limit: both planners solve well under all problems (about 85%), so the success
+rate measures the search, not the easiness of the scenes.
+Criteria, at 95%: the Wilson intervals of the two success rates overlap; the
+two-sample Kolmogorov-Smirnov test does not reject equal path-cost
+distributions; the bootstrap intervals of the two median costs overlap.  Every
+GPU path is re-validated with the float64 binary checker at 0.01 rad.
+
+PRRTC_DIST_PROBLEMS sets the problem count (default 1000).
 """
 from __future__ import annotations
 
@@ -22,22 +29,23 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 N_PROBLEMS = int(os.environ.get("PRRTC_DIST_PROBLEMS", "1000"))
-SETTINGS = dict(max_iterations=2000, step_size=0.5, num_new_samples=32, granularity=16, balance_mode=1,
+SETTINGS = dict(max_iterations=300, step_size=0.5, num_new_samples=32, granularity=16, balance_mode=1,
                 tree_ratio=0.5, dynamic_domain=True, collision_margin=0.02)
 CHECKER, MODE, RES, N_NODES = "binary_coarse_coop", 3, 0.01, 16384
+KIND = "dense"
 
 
 def _make(seed):
     from conftest import make_problem
 
-    return make_problem("tabletop", seed)
+    return make_problem(KIND, seed)
 
 
 def _oracle_plan(seed):
     from conftest import make_problem
     from oracle import oracle as O
 
-    pr = make_problem("tabletop", seed)
+    pr = make_problem(KIND, seed)
     sc = O.Scene(pr.context, pr.dim)
     r = O.plan(sc, pr.start, pr.goals, pr.lower, pr.upper, max_nodes=N_NODES, collision_mode=MODE,
                edge_resolution=RES, **SETTINGS)
@@ -66,7 +74,11 @@ def test_success_and_cost_distributions_match_oracle(cuda, orc):
     with ctx.Pool(max(1, min(32, os.cpu_count() or 1))) as pool:
         problems = pool.map(_make, seeds, chunksize=8)
         ora = pool.map(_oracle_plan, seeds, chunksize=8)
-    res = prrtc_plan_batch(np.stack([p.start for p in problems]), np.stack([p.goals for p in problems]),
+    G = max(p.goals.shape[0] for p in problems)
+    goals = np.zeros((len(problems), G, problems[0].dim), np.float32)
+    for i, p in enumerate(problems):
+        goals[i, : p.goals.shape[0]] = p.goals
+    res = prrtc_plan_batch(np.stack([p.start for p in problems]), goals, goal_counts=[p.goals.shape[0] for p in problems],
                            max_nodes=N_NODES, min_vals=problems[0].lower, max_vals=problems[0].upper,
                            collision_context=[p.context for p in problems], collision_checker=CHECKER,
                            edge_resolution=RES, return_trees=False, tail_explorers=False, **SETTINGS)
@@ -83,11 +95,18 @@ def test_success_and_cost_distributions_match_oracle(cuda, orc):
     assert bad == 0, f"{bad} paths failed re-validation"
     lo_g, hi_g = wilson(gs.sum(), gs.size)
     lo_o, hi_o = wilson(os_.sum(), os_.size)
-    assert lo_g <= hi_o and lo_o <= hi_g, f"success GPU {gs.mean():.3f} [{lo_g:.3f},{hi_g:.3f}] vs oracle " \
-                                          f"{os_.mean():.3f} [{lo_o:.3f},{hi_o:.3f}]"
+    summary = (f"success GPU {gs.mean():.4f} [{lo_g:.3f},{hi_g:.3f}] oracle {os_.mean():.4f} [{lo_o:.3f},{hi_o:.3f}]; "
+               f"median cost GPU {np.median(gc):.3f} oracle {np.median(oc):.3f}; "
+               f"mean cost GPU {gc.mean():.3f} oracle {oc.mean():.3f}")
+    print("\n" + summary)
+    # the workload discriminates: neither planner solves (almost) everything
+    assert 0.5 < os_.mean() < 0.97, summary
+    assert lo_g <= hi_o and lo_o <= hi_g, summary
+    from scipy.stats import ks_2samp
+
+    ks = ks_2samp(gc, oc)
+    assert ks.pvalue > 0.05, f"{summary}; KS D = {ks.statistic:.4f}, p = {ks.pvalue:.4f}"
     rng = np.random.default_rng(0)
     cg, co = boot_median(gc, rng), boot_median(oc, rng)
-    assert cg[0] <= co[1] and co[0] <= cg[1], f"median cost GPU {np.median(gc):.3f} {cg} vs oracle " \
-                                              f"{np.median(oc):.3f} {co}"
-    print(f"\nsuccess GPU {gs.mean():.4f} oracle {os_.mean():.4f}; median cost GPU {np.median(gc):.3f} {cg} "
-          f"oracle {np.median(oc):.3f} {co}; mean cost GPU {gc.mean():.3f} oracle {oc.mean():.3f}")
+    assert cg[0] <= co[1] and co[0] <= cg[1], f"{summary}; median cost intervals GPU {cg} oracle {co}"
+    print(f"KS D = {ks.statistic:.4f}, p = {ks.pvalue:.4f}; median cost intervals GPU {cg} oracle {co}")

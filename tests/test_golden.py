@@ -62,3 +62,35 @@ def test_connect_vectors(orc, gold):
         assert ne == int(gold[f"conn{k}_next"][0])
         vec = ((tree[:, idx] - cand) / np.float32(ne)).astype(np.float32) if ne else np.zeros(dim, np.float32)
         assert np.array_equal(bits(vec), bits(gold[f"conn{k}_vec"]))
+
+
+def _need(gold, key):
+    if key not in gold.files:
+        pytest.fail(f"{GOLDEN.name} lacks {key}: regenerate it with tests/golden/make_golden.py on a GPU")
+
+
+def test_tree_balance(orc, gold):
+    """Tree-side balance, all four modes, against the reference's own lines
+    (prrtc_planner.cu:790-824) run on a B200."""
+    from make_golden import BALANCE_TRIALS, balance_inputs
+
+    _need(gold, "bal0_tree")
+    for k in range(BALANCE_TRIALS):
+        mode, nb, ratio, sizes, li, vamp = balance_inputs(k)
+        tree, v = orc.choose_tree(mode, sizes, li, vamp, nb, ratio)
+        assert np.array_equal(tree, gold[f"bal{k}_tree"]), k
+        assert np.array_equal(v, gold[f"bal{k}_vamp"]), k
+
+
+def test_dynamic_domain_radii(orc, gold):
+    """Shrink / grow sequences and contended updates against the reference's
+    own CAS loops (prrtc_planner.cu:46-83) run on a B200."""
+    from make_golden import CONTENTION_TRIALS, RADIUS_TRIALS, contention_inputs, radius_inputs
+
+    _need(gold, "rad0")
+    for k in range(RADIUS_TRIALS):
+        alpha, r0, rmin, radii, idx, op = radius_inputs(k)
+        assert np.array_equal(bits(orc.radius_updates(radii, idx, op, alpha, r0, rmin)), bits(gold[f"rad{k}"])), k
+    for k in range(CONTENTION_TRIALS):
+        alpha, r0, rmin, radii, idx, op = contention_inputs(k)
+        assert np.array_equal(bits(orc.radius_updates(radii, idx, op, alpha, r0, rmin)), bits(gold[f"radc{k}"])), k

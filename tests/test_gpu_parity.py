@@ -281,9 +281,8 @@ def test_plan_solves_and_revalidates(cuda, orc, kind, seed, checker):
                                                  ("per_problem", 128, 0), ("per_problem", 32, 0),
                                                  ("per_problem", 256, 0)])
 def test_batch_uneven_solves(cuda, orc, launch, threads, ctas):
-    """threads=32 with the persistent launch runs one explorer per warp, four
-    explorers of a problem per CTA; ctas=2 caps the persistent grid at two CTAs
-    per SM with the smaller shared-memory carve-out."""
+    """threads=32 runs one-warp explorer CTAs; ctas=2 caps the persistent grid
+    at two CTAs per SM with the smaller shared-memory carve-out."""
     from prrtc_b200 import prrtc_plan_batch
 
     probs = [make_problem("uneven", 100 + i) for i in range(12)]
@@ -705,3 +704,66 @@ def test_more_than_32_joints(cuda, orc):
     assert r.solved
     ok, md = sc.validate_path(r.path.cpu().numpy(), 0.02)
     assert ok, md
+
+
+# ----------------------------------------------------------------------------- tree balance, dynamic domain
+
+def _golden_gen():
+    import sys as _sys
+
+    _sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import make_golden
+
+    return make_golden
+
+
+def test_choose_tree_matches_reference_and_oracle(cuda, orc):
+    """Tree-side balance, all four modes (prrtc_planner.cu:790-824): the
+    planner's device rule == the reference's own lines == the oracle, bit for
+    bit, for explorer counts 1-129, sizes around every switch of the rule, first
+    iterations and both mode-2 sides."""
+    from prrtc_b200 import _lib
+
+    lib, ref, g = _lib.load(), _ref(), _golden_gen()
+    ref.ref_balance.argtypes = [C.c_void_p] * 3 + [C.c_int] * 3 + [C.c_float] + [C.c_void_p] * 3
+    for k in range(g.BALANCE_TRIALS):
+        mode, nb, ratio, sizes, li, vamp = g.balance_inputs(k)
+        t_s, t_l, t_v = (torch.from_numpy(x).to(cuda) for x in (sizes, li, vamp))
+        mine_t, mine_v = torch.empty_like(t_v), torch.empty_like(t_v)
+        ref_t, ref_v = torch.empty_like(t_v), torch.empty_like(t_v)
+        _lib.check(lib.prrtc_b200_choose_tree(mode, sizes.shape[0], t_s.data_ptr(), t_l.data_ptr(), t_v.data_ptr(), nb,
+                                              ratio, mine_t.data_ptr(), mine_v.data_ptr(), _s()),
+                   "prrtc_b200_choose_tree")
+        assert ref.ref_balance(t_s.data_ptr(), t_l.data_ptr(), t_v.data_ptr(), sizes.shape[0], nb, mode, ratio,
+                               ref_t.data_ptr(), ref_v.data_ptr(), _s()) == 0
+        ora_t, ora_v = orc.choose_tree(mode, sizes, li, vamp, nb, ratio)
+        assert np.array_equal(ref_t.cpu().numpy(), ora_t), f"reference vs oracle, case {k}"
+        assert np.array_equal(ref_v.cpu().numpy(), ora_v), f"reference vs oracle mode-2 side, case {k}"
+        assert np.array_equal(mine_t.cpu().numpy(), ora_t), f"planner rule vs oracle, case {k}"
+        assert np.array_equal(mine_v.cpu().numpy(), ora_v), f"planner rule vs oracle mode-2 side, case {k}"
+
+
+def test_radius_updates_match_reference_and_oracle(cuda, orc):
+    """Dynamic-domain shrink / grow (prrtc_planner.cu:46-83): update sequences
+    applied in order, and 1024 concurrent updates contending on four nodes (one
+    kind per node, so the result does not depend on the CAS order): the
+    planner's device loops == the reference's own loops == the oracle, bit for
+    bit, from unset (FLT_MAX), clamped (rmin) and infinite radii."""
+    from prrtc_b200 import _lib
+
+    lib, ref, g = _lib.load(), _ref(), _golden_gen()
+    ref.ref_radius.argtypes = [C.c_void_p] * 3 + [C.c_int, C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]
+    err = torch.zeros(1, dtype=torch.int32, device=cuda)
+    cases = [(g.radius_inputs(k), 1) for k in range(g.RADIUS_TRIALS)] + \
+            [(g.contention_inputs(k), 0) for k in range(g.CONTENTION_TRIALS)]
+    for (alpha, r0, rmin, radii, idx, op), seq in cases:
+        t_i, t_o = torch.from_numpy(idx).to(cuda), torch.from_numpy(op).to(cuda)
+        mine, theirs = torch.from_numpy(radii).to(cuda), torch.from_numpy(radii).to(cuda)
+        _lib.check(lib.prrtc_b200_radius_update(mine.data_ptr(), t_i.data_ptr(), t_o.data_ptr(), idx.shape[0], alpha,
+                                                r0, rmin, seq, err.data_ptr(), _s()), "prrtc_b200_radius_update")
+        assert ref.ref_radius(theirs.data_ptr(), t_i.data_ptr(), t_o.data_ptr(), idx.shape[0], alpha, r0, rmin, seq,
+                              _s()) == 0
+        want = orc.radius_updates(radii, idx, op, alpha, r0, rmin)
+        assert np.array_equal(_bits(theirs.cpu().numpy()), _bits(want)), ("reference vs oracle", seq)
+        assert np.array_equal(_bits(mine.cpu().numpy()), _bits(want)), ("planner loops vs oracle", seq)
+    assert int(err.item()) == 0
