@@ -82,6 +82,9 @@ def parse():
                          "GPU and CPU path), 2 (1000 tabletop plans), 4 (smoothing of config-2 paths), 5 (1024 "
                          "dual-arm plans + smoothing), dense (the 512-problem batch at the 16-sphere scene's "
                          "density); 'none' skips them")
+    ap.add_argument("--split", choices=["weak", "strong"], default="weak",
+                    help="multi-GPU: every rank solves its own batch (weak) or one batch is split across ranks by "
+                         "longest-processing-time on estimated cost (strong)")
     ap.add_argument("--config5-problems", type=int, default=1024)
     ap.add_argument("--config2-problems", type=int, default=1000)
     return ap.parse_args()
@@ -96,11 +99,25 @@ def dist_env():
 
 # ----------------------------------------------------------------------------- workload
 
-def make_workload(n, rank, checker):
+def make_workload(n, rank, checker, split="weak", world=1):
+    """The uneven batch of `n` problems: rank r's own seeds (weak scaling), or
+    rank r's longest-processing-time share of one common batch (strong), the
+    cost of a problem estimated by its collision work times its tree capacity."""
     from prrtc_b200 import scenes
+    from prrtc_b200.shard import lpt_partition
 
     robot = scenes.arm(0)
-    return [scenes.make_problem("uneven", 100000 * (rank + 1) + i, checker, robot=robot) for i in range(n)]
+    if split == "weak":
+        return [scenes.make_problem("uneven", 100000 * (rank + 1) + i, checker, robot=robot) for i in range(n)]
+    allp = [scenes.make_problem("uneven", 100000 + i, checker, robot=robot) for i in range(n)]
+    return [allp[i] for i in lpt_partition([problem_cost(p) for p in allp], world)[rank]]
+
+
+def problem_cost(p):
+    c = p.context
+    work = sum(w * (0 if c.get(k) is None else len(c[k])) for k, w in (
+        ("world_spheres", 1.0), ("world_capsules", 2.0), ("world_boxes", 3.0), ("world_halfspaces", 1.0)))
+    return (1.0 + work) * p.max_nodes / 4096.0
 
 
 def oracle_checker(configs, ctx):
@@ -307,7 +324,7 @@ def run_ours(a):
 
     build.build()
     lib = _lib.load()
-    problems = make_workload(a.problems, rank, gpu_checker(dev))
+    problems = make_workload(a.problems, rank, gpu_checker(dev), a.split, ws)
     settings = PlanSettings()
     from prrtc_b200.autotune import choose, choose_joint
 
@@ -404,7 +421,7 @@ def run_ours(a):
 
     line = {
         "metric": METRIC, "value": value, "unit": "plans/s", "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": float(np.mean(step_ms)), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": float(np.mean(step_ms)), "higher_is_better": True, "scaling": a.split,
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "problems_per_gpu": len(problems),
                    "buckets": {str(N): len(ps) for N, ps in buckets.items()},
@@ -414,7 +431,10 @@ def run_ours(a):
                    "launch": ("eager" if a.eager else "CUDA graph replay") + (
                        ", one launch for all problems with per-problem tree capacities" if a.launch == "merged"
                        else ", one launch per capacity bucket on concurrent streams"),
-                   "parallelism": f"weak scaling, {ws} rank(s), problems sharded by rank"},
+                   "parallelism": (f"weak scaling, {ws} rank(s), every rank its own {len(problems)} problems"
+                                   if a.split == "weak" else
+                                   f"strong scaling, {ws} rank(s), one {a.problems}-problem batch split by "
+                                   "longest-processing-time on estimated cost")},
         "success_rate": success,
         "p50_solve_ms": float(np.median(solve_ms)) if solve_ms.size else None,
     }
@@ -550,15 +570,21 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     out.update(measure_nn(torch, dev, peaks))
     out.update(measure_smooth(torch, dev))
 
-    # --- CPU baseline (the reference's host loop restated), 1 core, bounded sample
+    # --- CPU baseline (the reference's host loop restated): Run A on one pinned
+    # core; Run B with a thread pool over each iteration's edge checks on every core
     from oracle import oracle as O
 
     O.build()
-    cb = cpu_baseline(problems, a.cpu_seconds, 1)
-    out["cpu_baseline"] = {"value": cb["plans_per_s"], "unit": "plans/s", "cores": 1, "kind": "port",
-                           "sample": f"first {cb['done']} problems of the workload in {cb['seconds']:.1f} s, "
-                                     f"host-driven RRT-Connect restated in C (prrtc_robogpu.py:103-298), "
-                                     f"{cpu_model()}"}
+    ra = _cpu_run(problems, 1, a.cpu_seconds, True)
+    rb = _cpu_run(problems, O.cpu_count(), a.cpu_seconds / 2, False)
+    out["cpu_baseline"] = {"value": ra["plans_per_s"], "unit": "plans/s", "cores": 1, "kind": "port",
+                           "sample": f"first {ra['problems']} problems of the workload ({a.cpu_seconds:.0f} s budget), "
+                                     f"one pinned core, host-driven RRT-Connect restated in C "
+                                     f"(prrtc_robogpu.py:103-298), {cpu_model()}"}
+    out["cpu_baseline_threads"] = {"value": rb["plans_per_s"], "unit": "plans/s", "cores": rb["threads"],
+                                   "sample": f"first {rb['problems']} problems, a thread pool over each iteration's "
+                                             f"edge checks on every core", "p50_solve_ms": rb["p50_solve_ms"],
+                                   "success_rate": rb["success_rate"]}
     return out
 
 

@@ -34,6 +34,10 @@
 
 namespace prrtc {
 
+#ifndef PRRTC_EXPLORE_MINBLOCKS
+#define PRRTC_EXPLORE_MINBLOCKS 2  // resident 256-thread explorer CTAs per SM the register allocation must allow
+#endif
+
 // ============================================================================ pack
 
 size_t blob_stride(const PackSrc& s) {
@@ -417,7 +421,7 @@ __device__ bool group_edge_collides(const Grp& grp, const Scene& sc, const CcBuf
     for (int c = 0; c < nchunk; ++c) {
         const int nw = (G - c + nchunk - 1) / nchunk;  // waypoints c, c+nchunk, ... below G
         const EdgeSrc e{base, delta, G, nchunk, c};
-        if (cc_chunk(grp, sc, B, nw, true, false, par, &e) != 0u) return true;
+        if (cc_chunk<false>(grp, sc, B, nw, true, par, &e) != 0u) return true;
     }
     return false;
 }
@@ -515,27 +519,31 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
             if (tid == 0 && L.dd) radius_shrink(P.radii[t], X.nn, L.dd_alpha, L.dd_radius, L.dd_min_radius, &L.queue[1]);
             continue;
         }
-        // insert (prrtc_planner.cu:925-947)
+        // insert (prrtc_planner.cu:925-947).  The other tree's size for the
+        // connect scan is read together with the slot claim (one round trip
+        // instead of two; any node published by then is scanned, as in the
+        // reference's read after its insert).  The nearest node's radius grows
+        // on another warp while the connect scan runs: nothing in this
+        // iteration reads it.
         if (tid == 0) {
+            const int so = ld_volatile(&P.sizes[o]);
             const int idx = atomicAdd(&P.sizes[t], 1);
             if (idx >= P.cap) {
                 if (atomicCAS(P.solved, 0, -1) == 0) stamp_end(P);
                 X.new_idx = -1;
             } else {
                 P.par[t][idx] = X.nn;
-                if (L.dd) radius_grow(P.radii[t], X.nn, L.dd_alpha, &L.queue[1]);
                 X.new_idx = idx;
             }
+            X.n_o = min(so, P.cap);
         }
         grp.sync();
         if (X.new_idx < 0) break;
         if (tid < dim) __stcg(&P.tree[t][(size_t)tid * N + X.new_idx], X.cand[tid]);
-        if (tid == 0) {
-            atomicAdd(&P.completed[t], 1);
-            X.n_o = min(ld_volatile(&P.sizes[o]), P.cap);
-        }
-        grp.sync();
-        // connect (prrtc_planner.cu:949-1043)
+        if (tid == 0) atomicAdd(&P.completed[t], 1);
+        if (L.dd && tid == (grp.size() > 32 ? 32 : 0)) radius_grow(P.radii[t], X.nn, L.dd_alpha, &L.queue[1]);
+        // connect (prrtc_planner.cu:949-1043); group_nearest's first barrier
+        // follows the scan, so X.cand / X.n_o written above are visible
         group_nearest(grp, P.tree[o], N, dim, X.n_o, X.cand, X.red_d, X.red_i);
         if (tid < 32) {
             const int lane = tid;
@@ -573,7 +581,11 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
             if (tid < 32) {
                 const int lane = tid;
                 int eidx = 0;
-                if (lane == 0) eidx = atomicAdd(&P.sizes[t], 1);
+                if (lane == 0) {
+                    // whether another explorer solved the problem meanwhile, read with the claim
+                    X.abort_ = ld_volatile(P.solved) != 0;
+                    eidx = atomicAdd(&P.sizes[t], 1);
+                }
                 eidx = __shfl_sync(0xffffffffu, eidx, 0);
                 if (eidx >= P.cap) {
                     if (lane == 0) {
@@ -592,11 +604,9 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
             grp.sync();
             if (X.ext_idx < 0) { failed = true; break; }
             if (tid < dim) __stcg(&P.tree[t][(size_t)tid * N + X.ext_idx], X.curr[tid]);
-            if (tid == 0) {
-                atomicAdd(&P.completed[t], 1);
-                X.abort_ = ld_volatile(P.solved) != 0;
-            }
-            grp.sync();
+            if (tid == 0) atomicAdd(&P.completed[t], 1);
+            // no barrier: the next sub-edge check only reads X.curr / X.vec, and
+            // warp 0 next writes them after that check's barriers
         }
         if (!failed) {  // connection found (prrtc_planner.cu:1045-1062)
             if (tid == 0) {
@@ -616,7 +626,7 @@ __device__ void run_explorer(const Grp& grp, const PlanLaunch& L, const Prob& P,
 
 // Plain form: grid = E explorers of problem blockIdx.y.  Persistent form: CTAs
 // pop (problem, explorer) slots until the queue is empty.
-__global__ void __launch_bounds__(256) explore_kernel(PlanLaunch L) {
+__global__ void __launch_bounds__(256, PRRTC_EXPLORE_MINBLOCKS) explore_kernel(PlanLaunch L) {
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ ExplorerSmem X;
     __shared__ __align__(8) uint64_t mbar;

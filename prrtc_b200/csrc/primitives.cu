@@ -298,11 +298,11 @@ cudaError_t launch_iteration(float* ta, float* tb, int32_t* pa, int32_t* pb, int
 #define PRRTC_CHECK_MINBLOCKS 4 // resident CTAs per SM the register allocation must allow (shared memory allows 4 at CW 32)
 #endif
 
-template <int CW>
+template <int CW, bool FULL>
 __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const unsigned char* __restrict__ gblob, int blob_cap,
                                                     const int32_t* pairs, int J, int S, int K, int Q, int dim,
-                                                    const float* __restrict__ configs, int n, int full_sweep,
-                                                    int32_t* verdicts, PcView pc) {
+                                                    const float* __restrict__ configs, int n, int32_t* verdicts,
+                                                    PcView pc) {
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ __align__(8) uint64_t mbar;
     const int tid = threadIdx.x;
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const
             B.q[w * kDimMax + d] = configs[(size_t)(c0 + w) * dim + d];
         }
         __syncthreads();
-        const uint32_t hit = cc_chunk(CtaGroup{}, sc, B, nw, false, full_sweep != 0, par);
+        const uint32_t hit = cc_chunk<FULL>(CtaGroup{}, sc, B, nw, false, par);
         for (int w = tid; w < nw; w += blockDim.x) verdicts[c0 + w] = (hit >> w) & 1u;
     }
 }
@@ -349,15 +349,14 @@ cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t*
         blob_cap = 0;
         dyn = cc;
     }
-    cudaError_t e = cudaFuncSetAttribute(check_kernel<CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    auto kern = full_sweep ? check_kernel<CW, true> : check_kernel<CW, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, check_kernel<CW>, 128, dyn)) != cudaSuccess)
-        return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, dyn)) != cudaSuccess) return e;
     const long long chunks = (n + CW - 1) / CW;
     const long long grid = std::min<long long>(chunks, (long long)std::max(per_sm, 1) * device_sm_count());
-    check_kernel<CW><<<(unsigned)grid, 128, dyn, st>>>(blob, blob_cap, pairs, J, S, K, Q, dim, configs, n,
-                                                        full_sweep, verdicts, cloud);
+    kern<<<(unsigned)grid, 128, dyn, st>>>(blob, blob_cap, pairs, J, S, K, Q, dim, configs, n, verdicts, cloud);
     return cudaGetLastError();
 }
 

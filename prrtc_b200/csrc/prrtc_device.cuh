@@ -36,6 +36,9 @@ constexpr int kSphChunk = PRRTC_SPH_CHUNK;  // fine spheres held in registers pe
 #ifndef PRRTC_PACKED_SWEEP
 #define PRRTC_PACKED_SWEEP 1  // full sweeps run the pair-wise (f32x2) primitive tests
 #endif
+#ifndef PRRTC_PACKED_EARLY_EXIT
+#define PRRTC_PACKED_EARLY_EXIT 0  // early-exit sweeps (planner edges) run them too
+#endif
 constexpr int kPairChunk = 32;   // explicit self pairs per work item
 constexpr float kFar = 1.0e18f;  // centre of a sphere that can never collide
 // Box records are stored scaled by 1/kBoxScale (a power of two, so the scaling
@@ -775,12 +778,15 @@ __device__ __forceinline__ SphPairs sph_pairs(const float4 (&s)[8]) {
     return p;
 }
 
-// Full sweep of obstacles [j0, j1) of the combined list against 8 spheres with
-// the packed tests: the same per-lane arithmetic (operand order, rounding) as
-// h_sphere / h_capsule / h_box / h_halfspace and the same thresholds, two
-// spheres per instruction, so the running minima and the verdicts are those of
-// obstacles_vs_spheres<8, true>.  Only the sphere pairs stay live (thresholds
-// are recomputed from them per primitive type).
+// Obstacles [j0, j1) of the combined list against 8 spheres with the packed
+// tests: the same per-lane arithmetic (operand order, rounding) as h_sphere /
+// h_capsule / h_box / h_halfspace and the same thresholds, two spheres per
+// instruction, so the running minima and the verdicts are those of the scalar
+// sweep.  FULL: every obstacle; otherwise the sweep stops at the first group of
+// kHitCheck obstacles that holds a hit (the mask is then non-zero but may be
+// incomplete).  Only the sphere pairs stay live (thresholds are recomputed from
+// them per primitive type).
+template <bool FULL>
 __device__ __forceinline__ uint32_t obstacles_vs_spheres_x2(const Scene& sc, int j0, int j1, const SphPairs& P,
                                                             int ns_real, unsigned long long& flops) {
     const BlobHeader& h = *sc.h;
@@ -823,6 +829,10 @@ __device__ __forceinline__ uint32_t obstacles_vs_spheres_x2(const Scene& sc, int
                 m[2 * j] = fmin3(m[2 * j], lo2(v1), lo2(v2));
                 m[2 * j + 1] = fmin3(m[2 * j + 1], hi2(v1), hi2(v2));
             }
+            if (!FULL && ((o - lo) & (kHitCheck - 1)) >= kHitCheck - 2 && any_le(m, thr)) {
+                flops += (unsigned long long)(o + 2 - lo) * ns_real * kFlopSphere;
+                return le_mask(m, thr);
+            }
         }
         if (o < hi) {  // the first obstacle of the last pair
             const ulonglong2* q = sc.pk_ws + 5 * (o >> 1);
@@ -830,6 +840,7 @@ __device__ __forceinline__ uint32_t obstacles_vs_spheres_x2(const Scene& sc, int
         }
         mask |= le_mask(m, thr);
         flops += (unsigned long long)(hi - lo) * ns_real * kFlopSphere;
+        if (!FULL && mask) return mask;
     }
     // capsules: t = sat(dp.(c, 1)), e = (c - p1) + t (-d), h = |e|^2 - (r_c + r)^2 against 0
     int base = h.Ns;
@@ -858,9 +869,14 @@ __device__ __forceinline__ uint32_t obstacles_vs_spheres_x2(const Scene& sc, int
                 m[2 * j] = fminf(m[2 * j], lo2(v));
                 m[2 * j + 1] = fminf(m[2 * j + 1], hi2(v));
             }
+            if (!FULL && ((o - lo) & (kHitCheck - 1)) == kHitCheck - 1 && any_le(m, thr)) {
+                flops += (unsigned long long)(o + 1 - lo) * ns_real * kFlopCapsule;
+                return le_mask(m, thr);
+            }
         }
         mask |= le_mask(m, thr);
         flops += (unsigned long long)(hi - lo) * ns_real * kFlopCapsule;
+        if (!FULL && mask) return mask;
     }
     // boxes (scaled by 1/kBoxScale): q_k = sat(|a_k.(c, 1)| - h_k), h = |q|^2 against (r/kBoxScale)^2
     base += h.Nc;
@@ -894,9 +910,14 @@ __device__ __forceinline__ uint32_t obstacles_vs_spheres_x2(const Scene& sc, int
                 m[2 * j] = fminf(m[2 * j], lo2(v));
                 m[2 * j + 1] = fminf(m[2 * j + 1], hi2(v));
             }
+            if (!FULL && ((o - lo) & (kHitCheck - 1)) == kHitCheck - 1 && any_le(m, thr)) {
+                flops += (unsigned long long)(o + 1 - lo) * ns_real * kFlopBox;
+                return le_mask(m, thr);
+            }
         }
         mask |= le_mask(m, thr);
         flops += (unsigned long long)(hi - lo) * ns_real * kFlopBox;
+        if (!FULL && mask) return mask;
     }
     // halfspaces (few per scene): h = n.c - n.p against r
     base += h.Nb;
@@ -934,7 +955,10 @@ template <int NS, bool FULL, bool PAIRS = FULL>
 __device__ __forceinline__ uint32_t obstacles_vs_spheres(const Scene& sc, int j0, int j1, const float4 (&s)[NS],
                                                          int ns_real, unsigned long long& flops) {
 #if PRRTC_PACKED_SWEEP
-    if constexpr (FULL && PAIRS && NS == 8) return obstacles_vs_spheres_x2(sc, j0, j1, sph_pairs(s), ns_real, flops);
+    if constexpr (FULL && PAIRS && NS == 8) return obstacles_vs_spheres_x2<true>(sc, j0, j1, sph_pairs(s), ns_real, flops);
+#endif
+#if PRRTC_PACKED_EARLY_EXIT
+    if constexpr (!FULL && NS == 8) return obstacles_vs_spheres_x2<false>(sc, j0, j1, sph_pairs(s), ns_real, flops);
 #endif
     const BlobHeader& h = *sc.h;
     float m[NS], thr[NS];
@@ -1098,9 +1122,10 @@ __device__ __forceinline__ float cc_joint_value(const JointRec& jr, const CcBufs
 // (the whole edge is rejected).  Otherwise each configuration stops at its own
 // first hit, or never with full_sweep.  Returns the hit bit mask (bit w =
 // configuration w in collision).
-template <class G>
-__device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B, int nw, bool edge_mode,
-                                    bool full_sweep, int& par, const EdgeSrc* edge = nullptr) {
+template <bool FULL_SWEEP, class G>
+__device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B, int nw, bool edge_mode, int& par,
+                                    const EdgeSrc* edge = nullptr) {
+    constexpr bool full_sweep = FULL_SWEEP;
     const BlobHeader& h = *sc.h;
     const int tid = g.rank(), T = g.size();
     const int J = h.J, S = h.S, S_pad = h.S_pad, K = h.K, Q = h.Q;

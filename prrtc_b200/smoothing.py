@@ -72,10 +72,27 @@ def smooth_cost(waypoints: torch.Tensor, sctx: SmoothContext) -> torch.Tensor:
 
 
 def resample_path(path: np.ndarray, W: int) -> np.ndarray:
-    """W waypoints evenly spaced in arc length along a piecewise-linear path."""
+    """W waypoints along a piecewise-linear path of L vertices.  With L <= W every
+    vertex is kept and the W - L extra points are spread over the segments in
+    proportion to their lengths (largest remainders first), so the resampled
+    polyline is the input path itself -- a smoothing pass that reverts returns
+    exactly the planner's path.  With L > W: W points evenly spaced in arc
+    length."""
     path = np.asarray(path, dtype=np.float64)
     if path.shape[0] == 1:
         return np.repeat(path, W, 0).astype(np.float32)
+    L = path.shape[0]
+    if L <= W:
+        seg = np.linalg.norm(np.diff(path, axis=0), axis=1)
+        extra = W - L
+        share = seg / seg.sum() * extra if seg.sum() > 0 else np.full(L - 1, extra / (L - 1))
+        n = np.floor(share).astype(np.int64)
+        rest = extra - int(n.sum())
+        if rest > 0:
+            n[np.argsort(-(share - n), kind="stable")[:rest]] += 1
+        out = [path[i] + (np.arange(n[i] + 1) / (n[i] + 1))[:, None] * (path[i + 1] - path[i]) for i in range(L - 1)]
+        out.append(path[-1:])
+        return np.concatenate(out, 0).astype(np.float32)
     seg = np.linalg.norm(np.diff(path, axis=0), axis=1)
     s = np.concatenate([[0.0], np.cumsum(seg)])
     if s[-1] <= 0:
@@ -113,6 +130,9 @@ def smooth_paths(paths: list, collision_context: dict, lower, upper, *, waypoint
                  resolution: float = 0.01, device=None):
     """Smooth each path (list of [L_i, dim] arrays) with projected gradient steps
     on the adjoint cost; re-validate at `resolution`; revert paths that fail.
+    A path of at most `waypoints` vertices reverts to itself (resample_path keeps
+    its vertices); for a longer one the reverted waypoints are its arc-length
+    resampling, and `accepted` tells the caller to keep the original path.
 
     Returns (smoothed [P, waypoints, dim] tensor, accepted [P] bool tensor,
     cost before [P], cost after [P])."""

@@ -132,3 +132,35 @@ def test_adjoint_mimic_dual_arm(cuda, orc):
     g = grad[0].cpu().numpy().astype(np.float64)
     rel = np.linalg.norm(g - g_ad) / np.linalg.norm(g_ad)
     assert rel < 1e-3, rel
+
+
+def test_batched_adjoint_each_path_in_its_own_world(cuda, orc):
+    """prrtc_b200_smooth_cost_grad_batch: path p against problem p's world (the
+    worlds differ in obstacle counts, so the packed tables are padded) gives the
+    cost and gradient of the single-scene entry point on that world, and the
+    cost of the float64 oracle; then the batched smoothing pass keeps only
+    paths that re-validate in their own world, and a reverted path is the
+    planner's path itself."""
+    from prrtc_b200.smoothing import BatchSmoothContext, SmoothContext, resample_path, smooth_paths_batch
+
+    cases = [_solved_path(orc, kind, seed) for kind, seed in (("tabletop", 3), ("uneven", 7), ("spheres16", 1),
+                                                            ("uneven", 11))]
+    W = 24
+    wps = np.stack([resample_path(path, W) for _, _, path in cases])
+    bctx = BatchSmoothContext([pr.context for pr, _, _ in cases], 7, MARGIN, BETA, WLEN, cuda)
+    cost_b, grad_b = bctx.cost_grad(torch.from_numpy(wps).to(cuda))
+    for i, (pr, sc, _) in enumerate(cases):
+        one = SmoothContext(pr.context, pr.dim, MARGIN, BETA, WLEN, cuda)
+        c1, g1 = one.cost_grad(torch.from_numpy(wps[i:i + 1]).to(cuda))
+        assert abs(cost_b[i].item() - c1.item()) <= 1e-5 * max(1.0, abs(c1.item())), i
+        assert torch.allclose(grad_b[i], g1[0], rtol=1e-5, atol=1e-6), i
+        c64 = sc.smooth_cost(wps[i].astype(np.float64), MARGIN, BETA, WLEN)
+        assert abs(cost_b[i].item() - c64) <= 1e-4 * max(1.0, abs(c64)), i
+    pr0 = cases[0][0]
+    out, acc, c0, c1 = smooth_paths_batch([path for _, _, path in cases], [pr.context for pr, _, _ in cases],
+                                          pr0.lower, pr0.upper, waypoints=32, steps=20, device=cuda)
+    for i, (pr, sc, path) in enumerate(cases):
+        ok, _ = sc.validate_path(out[i].cpu().numpy(), 0.01)
+        assert ok, i
+        if not bool(acc[i]):
+            assert np.array_equal(out[i].cpu().numpy(), resample_path(path, 32))

@@ -57,3 +57,17 @@ def test_two_rank_reduction_gloo():
     assert sorted(out[0][1] + out[1][1]) == list(range(40))
     assert all(o[2] == 2.0 for o in out)        # max of 1.0, 2.0
     assert all(o[3] == 40 for o in out)         # all problems counted once
+
+
+def test_strong_split_shares_one_batch():
+    """bench --split strong: the ranks' longest-processing-time shares of one
+    common batch are disjoint and cover it."""
+    import bench
+    from conftest import oracle_checker
+
+    shares = [bench.make_workload(16, r, oracle_checker, "strong", 2) for r in range(2)]
+    seeds = [sorted(p.seed for p in s) for s in shares]
+    assert not set(seeds[0]) & set(seeds[1])
+    assert sorted(seeds[0] + seeds[1]) == list(range(100000, 100016))
+    costs = [sum(bench.problem_cost(p) for p in s) for s in shares]
+    assert max(costs) <= sum(costs) / 2 + max(bench.problem_cost(p) for s in shares for p in s)
