@@ -519,7 +519,8 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
                        # (dram__bytes.sum.per_second x gpu__time_duration, profiles/explore_kernel_uneven512_eager.md):
                        # the trees, radii and scenes live in L1/L2, so the planner hardly touches HBM
                        "traffic": 7.4e6, "traffic_unit": "bytes per launch (ncu)",
-                       "peak_source": "measured in bench.py by the FFMA probe (no FP32 entry in MEASURED_PEAKS.json)",
+                       "peak_source": "measured in bench.py, the faster of the scalar FFMA and packed fma.rn.f32x2 "
+                                      "probes (no FP32 entry in MEASURED_PEAKS.json)",
                        "note": "collision FLOPs actually executed (device counters) / planner time; the planner is "
                                "latency-bound by its dependent sample->NN->extend->check iterations"}
     out["planner_collision_checks_per_s"] = cfgs / (ms * 1e-3)
@@ -1264,19 +1265,25 @@ def measure_plain_device(torch, dev, problems, settings, n_streams=8):
 
 def measure_configs(a, torch, lib, dev, settings, tuned):
     """The other BASELINE configurations, rank 0, after the headline."""
+    from prrtc_b200.batch import PlanSettings
+
     want = set(x.strip() for x in a.configs.split(",")) - {"none", ""}
     out = {}
     tuned_one = next(iter(tuned.values()))
-    if "dense" in want:
-        from prrtc_b200.batch import PlanSettings
-
-        out.update(measure_dense(torch, dev, PlanSettings(**{**settings.__dict__, **tuned_one})))
-    if "1" in want:
-        out.update(measure_config1(torch, dev))
-    if "2" in want or "4" in want:
-        out.update(measure_config2_4(torch, dev, settings, "4" in want, n=a.config2_problems))
-    if "5" in want:
-        out.update(measure_config5(torch, dev, settings, tuned_one, n=a.config5_problems))
+    jobs = [("dense", "dense512", lambda: measure_dense(torch, dev, PlanSettings(**{**settings.__dict__, **tuned_one}))),
+            ("1", "config1_single_plan", lambda: measure_config1(torch, dev)),
+            ("2", "config2_tabletop", lambda: measure_config2_4(torch, dev, settings, "4" in want,
+                                                                 n=a.config2_problems)),
+            ("5", "config5_dual_arm", lambda: measure_config5(torch, dev, settings, tuned_one,
+                                                               n=a.config5_problems))]
+    for key, name, fn in jobs:
+        if key in want or (key == "2" and "4" in want):
+            try:  # one configuration failing is reported in the line instead of losing the headline
+                out.update(fn())
+            except Exception as exc:  # noqa: BLE001
+                out[name] = {"error": f"{type(exc).__name__}: {exc}"[:500]}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
     return out
 
 

@@ -129,44 +129,6 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
         const float* c = &wh[i * 6];
         o_wh[i] = make_float4(c[0], c[1], c[2], -(c[0] * c[3] + c[1] * c[4] + c[2] * c[5]));
     }
-    // packed copies for the pair-wise tests (layout at pk_bytes in prrtc_device.cuh),
-    // the same values as the plain records, each duplicated into a pair
-    float4* pk_s = reinterpret_cast<float4*>(blob + L.o_pk);
-    for (int i = tid; i < 2 * ((Ns + 1) / 2); i += T) {
-        const int p = i >> 1, half = i & 1;
-        float4 O = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        float B = INFINITY;  // pad: never a hit
-        if (i < Ns) {
-            const float x = ws[i * 4], y = ws[i * 4 + 1], z = ws[i * 4 + 2], r = ws[i * 4 + 3];
-            O = make_float4(-2.0f * x, -2.0f * y, -2.0f * z, -2.0f * r);
-            B = fmaf(x, x, fmaf(y, y, fmaf(z, z, -r * r)));
-        }
-        pk_s[5 * p + 2 * half] = make_float4(O.x, O.x, O.y, O.y);
-        pk_s[5 * p + 2 * half + 1] = make_float4(O.z, O.z, O.w, O.w);
-        reinterpret_cast<float2*>(&pk_s[5 * p + 4])[half] = make_float2(B, B);
-    }
-    float4* pk_c = reinterpret_cast<float4*>(blob + L.o_pk + pk_sphere_bytes(Ns));
-    for (int i = tid; i < Nc; i += T) {
-        const float4 p1r = o_wc[3 * i], dp = o_wc[3 * i + 1], d = o_wc[3 * i + 2];
-        pk_c[6 * i] = make_float4(dp.x, dp.x, dp.y, dp.y);
-        pk_c[6 * i + 1] = make_float4(dp.z, dp.z, dp.w, dp.w);
-        pk_c[6 * i + 2] = make_float4(p1r.x, p1r.x, p1r.y, p1r.y);
-        pk_c[6 * i + 3] = make_float4(p1r.z, p1r.z, p1r.w, p1r.w);
-        pk_c[6 * i + 4] = make_float4(-d.x, -d.x, -d.y, -d.y);
-        pk_c[6 * i + 5] = make_float4(-d.z, -d.z, -p1r.w, -p1r.w);
-    }
-    float4* pk_b = pk_c + 6 * Nc;
-    for (int i = tid; i < Nb; i += T) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float4 a = o_wb[4 * i + k];
-            pk_b[8 * i + 2 * k] = make_float4(a.x, a.x, a.y, a.y);
-            pk_b[8 * i + 2 * k + 1] = make_float4(a.z, a.z, a.w, a.w);
-        }
-        const float4 h = o_wb[4 * i + 3];
-        pk_b[8 * i + 6] = make_float4(h.x, h.x, h.y, h.y);
-        pk_b[8 * i + 7] = make_float4(h.z, h.z, 0.0f, 0.0f);
-    }
     int2* cp = reinterpret_cast<int2*>(blob + L.o_cpair);
     for (int q = tid; q < Q; q += T) cp[q] = make_int2(s.cpairs[2 * q], s.cpairs[2 * q + 1]);
     // dense-block detection: coarse pair q's range is the row-major product of
@@ -257,7 +219,7 @@ __global__ void pack_kernel(PackSrc s, unsigned char* blobs, size_t stride, int 
         hd.o_joint = L.o_joint; hd.o_sph = L.o_sph; hd.o_sfr = L.o_sfr; hd.o_grp = L.o_grp;
         hd.o_sch = L.o_sch; hd.o_ws = L.o_ws; hd.o_wc = L.o_wc; hd.o_wb = L.o_wb;
         hd.o_wh = L.o_wh; hd.o_item = L.o_item; hd.o_cpair = L.o_cpair; hd.used_bytes = L.bytes;
-        hd.P = P; hd.cap_bytes = cap; hd.error = overflow ? kBlobItemOverflow : 0; hd.o_pk = L.o_pk;
+        hd.P = P; hd.cap_bytes = cap; hd.error = overflow ? kBlobItemOverflow : 0; hd.pad0 = 0;
         *h = hd;
     }
 }

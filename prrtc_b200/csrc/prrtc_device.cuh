@@ -33,12 +33,6 @@ constexpr int kObsChunk = 32;    // world primitives per work item
 #define PRRTC_SPH_CHUNK 8
 #endif
 constexpr int kSphChunk = PRRTC_SPH_CHUNK;  // fine spheres held in registers per work item
-#ifndef PRRTC_PACKED_SWEEP
-#define PRRTC_PACKED_SWEEP 1  // full sweeps run the pair-wise (f32x2) primitive tests
-#endif
-#ifndef PRRTC_PACKED_EARLY_EXIT
-#define PRRTC_PACKED_EARLY_EXIT 0  // early-exit sweeps (planner edges) run them too
-#endif
 constexpr int kPairChunk = 32;   // explicit self pairs per work item
 constexpr float kFar = 1.0e18f;  // centre of a sphere that can never collide
 // Box records are stored scaled by 1/kBoxScale (a power of two, so the scaling
@@ -69,7 +63,7 @@ struct BlobHeader {
     int32_t o_joint, o_sph, o_sfr, o_grp;
     int32_t o_sch, o_ws, o_wc, o_wb;
     int32_t o_wh, o_item, o_cpair, used_bytes;
-    int32_t P, cap_bytes, error, o_pk;
+    int32_t P, cap_bytes, error, pad0;
 };
 static_assert(sizeof(BlobHeader) == 128, "header must stay 128 bytes");
 // Bits of BlobHeader::error: the pack kernel's self-pair item list overflowed
@@ -92,24 +86,9 @@ __host__ __device__ inline int odd_pad(int s) { return s | 1; }
 // Capacity of a blob for the given (maximum) counts.  Layout offsets are
 // computed by the pack kernel with the same arithmetic.
 struct BlobLayout {
-    int o_joint, o_sph, o_sfr, o_grp, o_sch, o_ws, o_wc, o_wb, o_wh, o_item, o_cpair, o_pk, bytes;
+    int o_joint, o_sph, o_sfr, o_grp, o_sch, o_ws, o_wc, o_wb, o_wh, o_item, o_cpair, bytes;
     int sch_cap, item_cap;
 };
-
-// Packed copies of the world primitives for the pair-wise (fma.rn.f32x2) tests
-// of the full sweep, at o_pk: every operand duplicated into both halves of a
-// 64-bit pair, so one 128-bit shared-memory load yields two ready operands.
-//   spheres   80 B per pair of obstacles (2p, 2p+1): (Ox Ox Oy Oy) (Oz Oz Ow Ow) of
-//             each, then (B B B' B'); an odd count ends with a never-hit pad
-//             (O = 0, B = +inf)
-//   capsules  96 B each: (dp.x dp.x dp.y dp.y) (dp.z dp.z dp.w dp.w) (p1.x p1.x p1.y p1.y)
-//             (p1.z p1.z r r) (-d.x -d.x -d.y -d.y) (-d.z -d.z -r -r)
-//   boxes     128 B each: rows (a.x a.x a.y a.y) (a.z a.z a.w a.w) of the three axes,
-//             then (h1 h1 h2 h2) (h3 h3 0 0)   (scaled by 1/kBoxScale as the plain record)
-// Sub-section offsets follow from the actual counts: spheres at o_pk, capsules
-// at o_pk + 80 ceil(Ns/2), boxes after them.
-__host__ __device__ inline int pk_sphere_bytes(int Ns) { return 80 * ((Ns + 1) / 2); }
-__host__ __device__ inline int pk_bytes(int Ns, int Nc, int Nb) { return pk_sphere_bytes(Ns) + 96 * Nc + 128 * Nb; }
 
 __host__ __device__ inline BlobLayout blob_layout(int J, int S, int K, int Q, int P, int Ns, int Nc,
                                                   int Nb, int Nh) {
@@ -128,7 +107,6 @@ __host__ __device__ inline BlobLayout blob_layout(int J, int S, int K, int Q, in
     L.o_wh = off;    off += Nh * 16;
     L.o_item = off;  off += L.item_cap * 16;
     L.o_cpair = off; off += align16(Q * 8);
-    L.o_pk = off;    off += pk_bytes(Ns, Nc, Nb);
     L.bytes = align16(off);
     return L;
 }
@@ -156,9 +134,6 @@ struct Scene {  // typed view of a blob (shared or global memory)
     const int2* cpair;
     const int2* pairs;   // explicit self-pair list (global memory), for non-block items
     PcView pc;           // environment point cloud (global memory), pc.n == 0 when absent
-    const ulonglong2* pk_ws;  // packed spheres: 5 per obstacle pair
-    const ulonglong2* pk_wc;  // packed capsules: 6 each
-    const ulonglong2* pk_wb;  // packed boxes: 8 each
 };
 
 __device__ __forceinline__ Scene scene_view(const unsigned char* b) {
@@ -177,9 +152,6 @@ __device__ __forceinline__ Scene scene_view(const unsigned char* b) {
     s.cpair = reinterpret_cast<const int2*>(b + s.h->o_cpair);
     s.pairs = nullptr;
     s.pc = PcView{nullptr, nullptr, 0, 0, 0.0f, 0.0f};
-    s.pk_ws = reinterpret_cast<const ulonglong2*>(b + s.h->o_pk);
-    s.pk_wc = reinterpret_cast<const ulonglong2*>(b + s.h->o_pk + pk_sphere_bytes(s.h->Ns));
-    s.pk_wb = s.pk_wc + 6 * s.h->Nc;
     return s;
 }
 
@@ -718,248 +690,12 @@ __device__ __forceinline__ uint32_t le_mask(const float (&m)[NS], const float (&
     return r;
 }
 
-// ----------------------------------------------------------------------------- pair-wise (f32x2) tests
-
-// Two FP32 lanes in one 64-bit register pair, for sm_100's packed FP32
-// instructions (fma / add / sub / mul .rn.f32x2): one issue slot computes both
-// lanes, each lane rounded exactly as the scalar instruction.
-typedef unsigned long long f32x2;
-
-__device__ __forceinline__ f32x2 pk2(float lo, float hi) {
-    f32x2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ float lo2(f32x2 v) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    return a;
-}
-__device__ __forceinline__ float hi2(f32x2 v) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    return b;
-}
-__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
-    f32x2 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
-    f32x2 d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-
-// Eight sphere centres as four pairs per coordinate: pair j = spheres 2j, 2j+1.
-struct SphPairs {
-    f32x2 x[4], y[4], z[4], w[4];
-};
-
-__device__ __forceinline__ SphPairs sph_pairs(const float4 (&s)[8]) {
-    SphPairs p;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        p.x[j] = pk2(s[2 * j].x, s[2 * j + 1].x);
-        p.y[j] = pk2(s[2 * j].y, s[2 * j + 1].y);
-        p.z[j] = pk2(s[2 * j].z, s[2 * j + 1].z);
-        p.w[j] = pk2(s[2 * j].w, s[2 * j + 1].w);
-    }
-    return p;
-}
-
-// Obstacles [j0, j1) of the combined list against 8 spheres with the packed
-// tests: the same per-lane arithmetic (operand order, rounding) as h_sphere /
-// h_capsule / h_box / h_halfspace and the same thresholds, two spheres per
-// instruction, so the running minima and the verdicts are those of the scalar
-// sweep.  FULL: every obstacle; otherwise the sweep stops at the first group of
-// kHitCheck obstacles that holds a hit (the mask is then non-zero but may be
-// incomplete).  Only the sphere pairs stay live (thresholds are recomputed from
-// them per primitive type).
-template <bool FULL>
-__device__ __forceinline__ uint32_t obstacles_vs_spheres_x2(const Scene& sc, int j0, int j1, const SphPairs& P,
-                                                            int ns_real, unsigned long long& flops) {
-    const BlobHeader& h = *sc.h;
-    float m[8], thr[8];
-    uint32_t mask = 0u;
-    // spheres: h = B + O.(c, r) against -(|c|^2 - r^2); two obstacles per step
-    int lo = max(j0, 0), hi = min(j1, h.Ns);
-    if (lo < hi) {
-        const f32x2 zero = pk2(0.0f, 0.0f);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const f32x2 A = fma2(P.x[j], P.x[j], fma2(P.y[j], P.y[j], fma2(P.z[j], P.z[j],
-                                                                             mul2(sub2(zero, P.w[j]), P.w[j]))));
-            thr[2 * j] = -lo2(A);
-            thr[2 * j + 1] = -hi2(A);
-            m[2 * j] = m[2 * j + 1] = INFINITY;
-        }
-        auto one = [&](const ulonglong2 A, const ulonglong2 C, f32x2 B) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const f32x2 v = fma2(P.x[j], A.x, fma2(P.y[j], A.y, fma2(P.z[j], C.x, fma2(P.w[j], C.y, B))));
-                m[2 * j] = fminf(m[2 * j], lo2(v));
-                m[2 * j + 1] = fminf(m[2 * j + 1], hi2(v));
-            }
-        };
-        int o = lo;
-        if (o & 1) {  // odd start: the second obstacle of its pair alone
-            const ulonglong2* q = sc.pk_ws + 5 * (o >> 1);
-            one(q[2], q[3], q[4].y);
-            ++o;
-        }
-#pragma unroll 1
-        for (; o + 1 < hi; o += 2) {
-            const ulonglong2* q = sc.pk_ws + 5 * (o >> 1);
-            const ulonglong2 A1 = q[0], C1 = q[1], A2 = q[2], C2 = q[3], Bq = q[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const f32x2 v1 = fma2(P.x[j], A1.x, fma2(P.y[j], A1.y, fma2(P.z[j], C1.x, fma2(P.w[j], C1.y, Bq.x))));
-                const f32x2 v2 = fma2(P.x[j], A2.x, fma2(P.y[j], A2.y, fma2(P.z[j], C2.x, fma2(P.w[j], C2.y, Bq.y))));
-                m[2 * j] = fmin3(m[2 * j], lo2(v1), lo2(v2));
-                m[2 * j + 1] = fmin3(m[2 * j + 1], hi2(v1), hi2(v2));
-            }
-            if (!FULL && ((o - lo) & (kHitCheck - 1)) >= kHitCheck - 2 && any_le(m, thr)) {
-                flops += (unsigned long long)(o + 2 - lo) * ns_real * kFlopSphere;
-                return le_mask(m, thr);
-            }
-        }
-        if (o < hi) {  // the first obstacle of the last pair
-            const ulonglong2* q = sc.pk_ws + 5 * (o >> 1);
-            one(q[0], q[1], q[4].x);
-        }
-        mask |= le_mask(m, thr);
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopSphere;
-        if (!FULL && mask) return mask;
-    }
-    // capsules: t = sat(dp.(c, 1)), e = (c - p1) + t (-d), h = |e|^2 - (r_c + r)^2 against 0
-    int base = h.Ns;
-    lo = max(j0, base) - base;
-    hi = min(j1, base + h.Nc) - base;
-    if (lo < hi) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            thr[k] = 0.0f;
-            m[k] = INFINITY;
-        }
-#pragma unroll 1
-        for (int o = lo; o < hi; ++o) {
-            const ulonglong2* q = sc.pk_wc + 6 * o;
-            const ulonglong2 DP0 = q[0], DP1 = q[1], P0 = q[2], P1 = q[3], ND0 = q[4], ND1 = q[5];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const f32x2 tt = fma2(DP0.x, P.x[j], fma2(DP0.y, P.y[j], fma2(DP1.x, P.z[j], DP1.y)));
-                const f32x2 t = pk2(__saturatef(lo2(tt)), __saturatef(hi2(tt)));
-                const f32x2 ex = fma2(t, ND0.x, sub2(P.x[j], P0.x));
-                const f32x2 ey = fma2(t, ND0.y, sub2(P.y[j], P0.y));
-                const f32x2 ez = fma2(t, ND1.x, sub2(P.z[j], P1.x));
-                const f32x2 sr = add2(P.w[j], P1.y);    // r + r_c
-                const f32x2 nsr = sub2(ND1.y, P.w[j]);  // -(r + r_c), exactly
-                const f32x2 v = fma2(ex, ex, fma2(ey, ey, fma2(ez, ez, mul2(nsr, sr))));
-                m[2 * j] = fminf(m[2 * j], lo2(v));
-                m[2 * j + 1] = fminf(m[2 * j + 1], hi2(v));
-            }
-            if (!FULL && ((o - lo) & (kHitCheck - 1)) == kHitCheck - 1 && any_le(m, thr)) {
-                flops += (unsigned long long)(o + 1 - lo) * ns_real * kFlopCapsule;
-                return le_mask(m, thr);
-            }
-        }
-        mask |= le_mask(m, thr);
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopCapsule;
-        if (!FULL && mask) return mask;
-    }
-    // boxes (scaled by 1/kBoxScale): q_k = sat(|a_k.(c, 1)| - h_k), h = |q|^2 against (r/kBoxScale)^2
-    base += h.Nc;
-    lo = max(j0, base) - base;
-    hi = min(j1, base + h.Nb) - base;
-    if (lo < hi) {
-        const f32x2 inv = pk2(kBoxInv, kBoxInv);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const f32x2 rs = mul2(P.w[j], inv);
-            const f32x2 r2 = mul2(rs, rs);
-            thr[2 * j] = lo2(r2);
-            thr[2 * j + 1] = hi2(r2);
-            m[2 * j] = m[2 * j + 1] = INFINITY;
-        }
-#pragma unroll 1
-        for (int o = lo; o < hi; ++o) {
-            const ulonglong2* q = sc.pk_wb + 8 * o;
-            const ulonglong2 R0 = q[0], R1 = q[1], R2 = q[2], R3 = q[3], R4 = q[4], R5 = q[5];
-            const float4 HL = reinterpret_cast<const float4*>(q)[6];
-            const float4 HL3 = reinterpret_cast<const float4*>(q)[7];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const f32x2 l1 = fma2(R0.x, P.x[j], fma2(R0.y, P.y[j], fma2(R1.x, P.z[j], R1.y)));
-                const f32x2 l2 = fma2(R2.x, P.x[j], fma2(R2.y, P.y[j], fma2(R3.x, P.z[j], R3.y)));
-                const f32x2 l3 = fma2(R4.x, P.x[j], fma2(R4.y, P.y[j], fma2(R5.x, P.z[j], R5.y)));
-                const f32x2 q1 = pk2(__saturatef(fabsf(lo2(l1)) - HL.x), __saturatef(fabsf(hi2(l1)) - HL.x));
-                const f32x2 q2 = pk2(__saturatef(fabsf(lo2(l2)) - HL.z), __saturatef(fabsf(hi2(l2)) - HL.z));
-                const f32x2 q3 = pk2(__saturatef(fabsf(lo2(l3)) - HL3.x), __saturatef(fabsf(hi2(l3)) - HL3.x));
-                const f32x2 v = fma2(q1, q1, fma2(q2, q2, mul2(q3, q3)));
-                m[2 * j] = fminf(m[2 * j], lo2(v));
-                m[2 * j + 1] = fminf(m[2 * j + 1], hi2(v));
-            }
-            if (!FULL && ((o - lo) & (kHitCheck - 1)) == kHitCheck - 1 && any_le(m, thr)) {
-                flops += (unsigned long long)(o + 1 - lo) * ns_real * kFlopBox;
-                return le_mask(m, thr);
-            }
-        }
-        mask |= le_mask(m, thr);
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopBox;
-        if (!FULL && mask) return mask;
-    }
-    // halfspaces (few per scene): h = n.c - n.p against r
-    base += h.Nb;
-    lo = max(j0, base) - base;
-    hi = min(j1, base + h.Nh) - base;
-    if (lo < hi) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            thr[2 * j] = lo2(P.w[j]);
-            thr[2 * j + 1] = hi2(P.w[j]);
-            m[2 * j] = m[2 * j + 1] = INFINITY;
-        }
-#pragma unroll 1
-        for (int o = lo; o < hi; ++o) {
-            const float4 hs = sc.wh[o];
-            const f32x2 nx = pk2(hs.x, hs.x), ny = pk2(hs.y, hs.y), nz = pk2(hs.z, hs.z), nw = pk2(hs.w, hs.w);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const f32x2 v = fma2(nx, P.x[j], fma2(ny, P.y[j], fma2(nz, P.z[j], nw)));
-                m[2 * j] = fminf(m[2 * j], lo2(v));
-                m[2 * j + 1] = fminf(m[2 * j + 1], hi2(v));
-            }
-        }
-        mask |= le_mask(m, thr);
-        flops += (unsigned long long)(hi - lo) * ns_real * kFlopHalfspace;
-    }
-    return mask;
-}
-
 // Returns the spheres found in collision as a bit mask (bit k = s[k]).  With
 // !FULL the sweep stops at the first group of obstacles holding a hit, so the
-// mask is then non-zero but may be incomplete.  The throughput form (FULL and
-// PAIRS, 8 spheres) runs the pair-wise tests.
+// mask is then non-zero but may be incomplete.
 template <int NS, bool FULL, bool PAIRS = FULL>
 __device__ __forceinline__ uint32_t obstacles_vs_spheres(const Scene& sc, int j0, int j1, const float4 (&s)[NS],
                                                          int ns_real, unsigned long long& flops) {
-#if PRRTC_PACKED_SWEEP
-    if constexpr (FULL && PAIRS && NS == 8) return obstacles_vs_spheres_x2<true>(sc, j0, j1, sph_pairs(s), ns_real, flops);
-#endif
-#if PRRTC_PACKED_EARLY_EXIT
-    if constexpr (!FULL && NS == 8) return obstacles_vs_spheres_x2<false>(sc, j0, j1, sph_pairs(s), ns_real, flops);
-#endif
     const BlobHeader& h = *sc.h;
     float m[NS], thr[NS];
     uint32_t mask = 0u;
