@@ -439,8 +439,6 @@ def run_ours(a):
         "p50_solve_ms": float(np.median(solve_ms)) if solve_ms.size else None,
     }
     line["gpu_launches"] = 6 * len(planners) * a.steps  # per planner: fill, pack, init, explore, finalize, paths
-    if rank == 0 and not a.no_extras:
-        line.update(revalidate_step(planners))
 
     # e2e on every rank (each its own problems), whole job = all ranks' plans
     # over the slowest rank's seconds
@@ -464,6 +462,8 @@ def run_ours(a):
                               "rank's time)"}
 
     if rank == 0 and not a.no_extras:
+        # the planners' buffers still hold the last timed step (e2e plans into its own)
+        line.update(revalidate_step(planners))
         line.update(extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of))
         line.update(measure_configs(a, torch, lib, dev, settings, tuned))
     if rank == 0:

@@ -156,7 +156,8 @@ typedef struct {
     float edge_resolution;       /* >0: an edge gets max(granularity, ceil(len/res)) waypoints */
     int32_t threads_per_explorer;/* threads of one explorer (one explorer per CTA): 32, 64, 128
                                     or 256 (default 128) */
-    int32_t waypoint_chunk;      /* waypoints checked per CTA pass: 8, 16 or 32 (default 16) */
+    int32_t waypoint_chunk;      /* waypoints of an edge checked per CTA pass: 8, 16, 32 or 64
+                                    (default 16) */
     int32_t resident_ctas;       /* batched planner grid (default: all resident CTAs) */
     uint64_t* stats;             /* optional device counters [4], accumulated: edges checked,
                                     configurations checked, FP32 flops of the collision work

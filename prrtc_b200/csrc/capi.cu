@@ -113,7 +113,8 @@ static Tuned tuned(const prrtc_tuning_t* t) {
         if (t->threads_per_explorer == 32 || t->threads_per_explorer == 64 || t->threads_per_explorer == 128 ||
             t->threads_per_explorer == 256)
             o.threads = t->threads_per_explorer;
-        if (t->waypoint_chunk == 8 || t->waypoint_chunk == 16 || t->waypoint_chunk == 32) o.cw = t->waypoint_chunk;
+        if (t->waypoint_chunk == 8 || t->waypoint_chunk == 16 || t->waypoint_chunk == 32 || t->waypoint_chunk == 64)
+            o.cw = t->waypoint_chunk;
         if (t->resident_ctas > 0) o.resident = t->resident_ctas;
         o.stats = reinterpret_cast<unsigned long long*>(t->stats);
         o.cloud = t->point_cloud;

@@ -768,9 +768,10 @@ struct CcBufs {
     float4* cctr;    // [CW][K]
     uint32_t* dirty; // [CW][KW]
     uint32_t* gate;  // [CW][QW]
-    uint32_t* hit;   // [1]
+    uint32_t* hit;   // [4]: two alternating result words, two work-list counters
     int* bounds;     // [2][kMaxParts + 1] first obstacle of each world part (fine pass, coarse pass)
     unsigned long long* stats;  // optional device counters (kStat*), may be null
+    int listcap;     // ints the work lists may use in `pose` once the centres are placed
 };
 
 constexpr int kMaxParts = 256;  // world parts per chunk (cost-balanced obstacle ranges)
@@ -804,6 +805,7 @@ __device__ inline CcBufs cc_bufs(unsigned char* base, int J, int S, int K, int Q
     b.hit = reinterpret_cast<uint32_t*>(p);    p += 16;
     b.bounds = reinterpret_cast<int*>(p);
     b.stats = nullptr;
+    b.listcap = CW * J * 12;
     return b;
 }
 
@@ -967,7 +969,10 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     }
     g.sync();
     // every thread has read the other word's previous result by now
-    if (tid == 0) B.hit[par] = 0u;  // par was flipped: this is the word the next call uses
+    if (tid == 0) {
+        B.hit[par] = 0u;  // par was flipped: this is the word the next call uses
+        B.hit[2] = B.hit[3] = 0u;  // work-list counters
+    }
     unsigned long long flops = 0;
     // D: coarse pre-pass -> dirty groups and touching coarse self pairs
     if (gated) {
@@ -998,26 +1003,65 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         }
         g.sync();
     }
+    // E0 (gated early-exit checks): the coarse pass leaves only a few (sphere
+    // chunk, waypoint) pairs dirty and a few self items touching, and dealing all
+    // items out by index gave the few threads holding real work a long tail that
+    // the rest of the CTA waited for at the final barrier.  Compact the live
+    // pairs and items into lists (in `pose`, free once the centres are placed),
+    // then spread them: every dirty pair's obstacle list is cut into n_sub
+    // cost-balanced ranges so that the world work makes about two items per
+    // thread.
+    const bool compact = gated && !full_sweep && nw * (h.n_sch + h.n_items) <= B.listcap;
+    int* wl = reinterpret_cast<int*>(B.pose);  // (sphere chunk << 8 | waypoint) of dirty pairs
+    int* sl = wl + nw * h.n_sch;               // (self item << 8 | waypoint) of touching items
+    if (compact) {
+        for (int i = tid; i < nw * h.n_sch; i += T) {
+            const int si = i / nw, w = i - si * nw;
+            const int4 ch = sc.sch[si];
+            if (ch.z < 0 || (B.dirty[w * KW + (ch.z >> 5)] & (1u << (ch.z & 31)))) wl[atomicAdd(&B.hit[2], 1u)] = (si << 8) | w;
+        }
+        for (int i = tid; i < nw * h.n_items; i += T) {
+            const int ii = i / nw, w = i - ii * nw;
+            const int4 item = sc.item[ii];
+            if (item.w < 0 || (B.gate[w * QW + (item.w >> 5)] & (1u << (item.w & 31)))) sl[atomicAdd(&B.hit[3], 1u)] = (ii << 8) | w;
+        }
+        g.sync();
+    }
+    const int Lw = compact ? (int)B.hit[2] : 0, Ls = compact ? (int)B.hit[3] : 0;
+    const int n_sub = Lw > 0 ? min(max(1, cdiv(2 * T, Lw)), max(1, cdiv(n_obs, 4))) : 0;
     // E: fine work items.  World: (obstacle chunk, sphere chunk, waypoint) with the
-    // obstacle chunk slowest so a warp reads the same primitive (broadcast).
-    // Self: (item, waypoint).
-    const int n_world = nw * h.n_sch * n_parts;
-    const int n_self = nw * h.n_items;
+    // obstacle chunk slowest so a warp reads the same primitive (broadcast); from
+    // the list: (obstacle range, list entry), range slowest.  Self: (item,
+    // waypoint), or the listed ones.
+    const int n_world = compact ? Lw * n_sub : nw * h.n_sch * n_parts;
+    const int n_self = compact ? Ls : nw * h.n_items;
     const int n_total = n_world + n_self + (sc.pc.n > 0 ? nw * S : 0);
     auto run_item = [&](int it) {
         int w;
         bool hit = false;
         if (it < n_world) {
-            const int part = it / (nw * h.n_sch), r = it - part * (nw * h.n_sch);
-            const int si = r / nw;
-            w = r - si * nw;
-            if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) return;
+            int si, j0, j1;
+            if (compact) {
+                const int p = it / Lw, ent = wl[it - p * Lw];
+                si = ent >> 8;
+                w = ent & 255;
+                if (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u)) return;
+                j0 = world_index_at(h, (int)((long long)p * ctot / n_sub));
+                j1 = world_index_at(h, (int)((long long)(p + 1) * ctot / n_sub));
+            } else {
+                const int part = it / (nw * h.n_sch), r = it - part * (nw * h.n_sch);
+                si = r / nw;
+                w = r - si * nw;
+                if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) return;
+                const int4 chk = sc.sch[si];
+                if (gated && chk.z >= 0 && !(B.dirty[w * KW + (chk.z >> 5)] & (1u << (chk.z & 31)))) return;
+                j0 = B.bounds[part];
+                j1 = B.bounds[part + 1];
+            }
             const int4 ch = sc.sch[si];
-            if (gated && ch.z >= 0 && !(B.dirty[w * KW + (ch.z >> 5)] & (1u << (ch.z & 31)))) return;
             float4 s[kSphChunk];
 #pragma unroll
             for (int m = 0; m < kSphChunk; ++m) s[m] = (m < ch.y) ? B.ctr[w * S_pad + ch.x + m] : absent_sphere();
-            const int j0 = B.bounds[part], j1 = B.bounds[part + 1];
             hit = (full_sweep ? obstacles_vs_spheres<kSphChunk, true>(sc, j0, j1, s, ch.y, flops)
                               : obstacles_vs_spheres<kSphChunk, false>(sc, j0, j1, s, ch.y, flops)) != 0u;
         } else if (it >= n_world + n_self) {  // point cloud: (sphere, waypoint)
@@ -1028,11 +1072,18 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
             hit = pc_sphere_hits(sc.pc, B.ctr[w * S_pad + si], full_sweep, flops);
         } else {
             const int r = it - n_world;
-            const int ii = r / nw;
-            w = r - ii * nw;
+            int ii;
+            if (compact) {
+                const int ent = sl[r];
+                ii = ent >> 8;
+                w = ent & 255;
+            } else {
+                ii = r / nw;
+                w = r - ii * nw;
+            }
             if (!full_sweep && (edge_mode ? (*vhit != 0u) : ((*vhit >> w) & 1u))) return;
             const int4 item = sc.item[ii];
-            if (gated && item.w >= 0 && !(B.gate[w * QW + (item.w >> 5)] & (1u << (item.w & 31)))) return;
+            if (!compact && gated && item.w >= 0 && !(B.gate[w * QW + (item.w >> 5)] & (1u << (item.w & 31)))) return;
             const float4* C = &B.ctr[w * S_pad];
             if (item.y >= 0) {  // dense block: spheres [a0, a0+na) x [b0, b0+nb)
                 // self pairs use radius rho = r + inflate/2 per sphere, so the pair
@@ -1079,7 +1130,9 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         }
         // one shared-memory atomic per warp: OR the hit bits of the active lanes
         const unsigned active = __activemask();
-        const unsigned bits = __reduce_or_sync(active, hit ? (1u << w) : 0u);
+        // bit w per configuration (nw <= 32 outside edge mode); an edge only needs
+        // the word to become non-zero, which bit w & 31 does for chunks of 64
+        const unsigned bits = __reduce_or_sync(active, hit ? (1u << (w & 31)) : 0u);
         if (bits && (threadIdx.x & 31) == (__ffs(active) - 1)) atomicOr(hw, bits);
     };
     for (int it = tid; it < n_total; it += T) run_item(it);
