@@ -943,8 +943,24 @@ def _batch_line(torch, dev, problems, caps, settings, steps, label):
            "p50_solve_ms": float(np.median(kt[solved])) if solved.any() else None,
            "p95_solve_ms": float(np.percentile(kt[solved], 95)) if solved.any() else None,
            "planner_nn_gbs": nn_gbs,
+           "tuning": {"num_new_samples": settings.num_new_samples, "threads_per_explorer": settings.threads_per_explorer,
+                      "waypoint_chunk": settings.waypoint_chunk, "ctas_per_sm": settings.ctas_per_sm},
            "buckets": {str(c): int(sum(1 for x in caps if x == c)) for c in sorted(set(caps))}}
     return out, res
+
+
+def _tune_chunk(problems, settings, dev):
+    """The headline's explorers, threads and CTAs per SM with the waypoint chunk
+    chosen for this workload (dense scenes reject most edges in the first pass
+    of a small chunk; sparse ones pass whole edges in one pass of 64)."""
+    from prrtc_b200.autotune import choose
+    from prrtc_b200.batch import PlanSettings
+
+    s = settings
+    cands = [(s.num_new_samples, s.threads_per_explorer, cw, s.ctas_per_sm) for cw in (16, 32, 64)]
+    best = choose(problems, [p.max_nodes for p in problems], s, dev, candidates=cands, use_cache=False, finalists=2,
+                  final_reps=2)
+    return PlanSettings(**{**s.__dict__, **best})
 
 
 def measure_dense(torch, dev, settings, steps=5, n=512):
@@ -960,6 +976,7 @@ def measure_dense(torch, dev, settings, steps=5, n=512):
     t0 = time.perf_counter()
     problems = [scenes.make_problem("dense", 300000 + i, chk, robot=robot) for i in range(n)]
     gen_s = time.perf_counter() - t0
+    settings = _tune_chunk(problems, settings, dev)
     out, _ = _batch_line(torch, dev, problems, [p.max_nodes for p in problems], settings, steps,
                          "dense512: the uneven counts (4-128 spheres r 0.05-0.15, 0-32 boxes of half extents "
                          "0.02-0.3 m) in [-0.8,0.8]^2 x [0,1.2], 1-8 goals, buckets 4096/16384/65536")
@@ -1173,7 +1190,7 @@ def measure_config5(torch, dev, settings, tuned, n=1024, steps=3):
     t0 = time.perf_counter()
     problems = [scenes.make_problem("large", 400000 + i, chk, robot=robot) for i in range(n)]
     gen_s = time.perf_counter() - t0
-    s = PlanSettings(**{**settings.__dict__, **tuned})
+    s = _tune_chunk(problems, PlanSettings(**{**settings.__dict__, **tuned}), dev)
     line, res = _batch_line(torch, dev, problems, [p.max_nodes for p in problems], s, steps,
                             f"{n} dual-arm problems (14 DOF + 4 mimic joints, 120 spheres), 256 spheres + 64 boxes "
                             "+ floor, 1-4 goals, 131072 nodes")

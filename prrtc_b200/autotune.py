@@ -18,7 +18,7 @@ import torch
 
 SAMPLES = (1, 2, 4, 8, 16)
 THREADS = (64, 128, 256)  # 32 stays available (a one-warp CTA) but is slower on every bucket measured
-CHUNKS = (8, 16, 32)
+CHUNKS = (8, 16, 32, 64)  # 64: one pass for most edges of a 0.5 rad step at 0.01 rad resolution
 CTAS_PER_SM = (0, 2)  # 0: as many as fit; 2: two, with the rest of shared memory given to L1
 CANDIDATES = tuple((e, t, c, r) for r in CTAS_PER_SM for t in THREADS for c in CHUNKS for e in SAMPLES)
 CACHE = Path(os.environ.get("PRRTC_B200_CACHE", Path.home() / ".cache" / "prrtc_b200")) / "autotune.json"
@@ -65,7 +65,7 @@ def choose(problems, N, settings, dev, candidates=CANDIDATES, use_cache: bool = 
     launches wins."""
     from .batch import BatchPlanner, PlanSettings
 
-    key = "v9|" + _key(dev, N, problems, settings)
+    key = "v10|" + _key(dev, N, problems, settings)
     cache = _load() if use_cache else {}
     if key in cache:
         return dict(cache[key])

@@ -8,9 +8,14 @@ The batched planner runs with exactly num_new_samples explorers per problem
 
 Workload: the dense uneven scenes (4-128 spheres and 0-32 boxes of half extents
 up to 0.3 m in [-0.8,0.8]^2 x [0,1.2]), where 2-25% of configuration space is
-free and some start / goal pairs are disconnected, with a tight iteration
-limit: both planners solve well under all problems (about 85%), so the success
-rate measures the search, not the easiness of the scenes.
+free and some start / goal pairs are disconnected, with a small tree capacity
+(512 nodes) and an iteration limit that is never reached: a problem ends when
+it connects or when a tree overflows, both planners solve well under all
+problems (about 90%), and the success rate measures the search, not the
+easiness of the scenes.  (Ending problems by the iteration limit instead would
+compare unlike things: on the GPU the first explorer to pass the limit ends the
+problem while its racing peers have run fewer iterations, where the round-robin
+restatement gives every explorer the full count.)
 Criteria, at 95%: the Wilson intervals of the two success rates overlap, and a
 one-sided two-sample Kolmogorov-Smirnov test does not find the GPU's path costs
 stochastically larger than the oracle's.  The cost test is one-sided on
@@ -42,9 +47,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 N_PROBLEMS = int(os.environ.get("PRRTC_DIST_PROBLEMS", "1000"))
-SETTINGS = dict(max_iterations=300, step_size=0.5, num_new_samples=32, granularity=16, balance_mode=1,
+SETTINGS = dict(max_iterations=5000, step_size=0.5, num_new_samples=32, granularity=16, balance_mode=1,
                 tree_ratio=0.5, dynamic_domain=True, collision_margin=0.02)
-CHECKER, MODE, RES, N_NODES = "binary_coarse_coop", 3, 0.01, 16384
+CHECKER, MODE, RES, N_NODES = "binary_coarse_coop", 3, 0.01, 512
 KIND = "dense"
 
 
