@@ -427,7 +427,7 @@ def run_ours(a):
                    "buckets": {str(N): len(ps) for N, ps in buckets.items()},
                    "tuned": {str(N): v for N, v in tuned.items()},
                    "collision_checker": settings.collision_checker, "edge_resolution": settings.edge_resolution,
-                   "threads_per_explorer": settings.threads_per_explorer, "l2": "flushed (256 MB write) between steps",
+                   "l2": "flushed (256 MB write) between steps",
                    "launch": ("eager" if a.eager else "CUDA graph replay") + (
                        ", one launch for all problems with per-problem tree capacities" if a.launch == "merged"
                        else ", one launch per capacity bucket on concurrent streams"),
