@@ -21,6 +21,9 @@
  *   prrtc_b200_iteration         <- PrrtcIterationImpl / "prrtc_iteration" (legacy)
  *                                   cuda-rrtc/CUDA/prrtc_extend.cu:76-140
  *   prrtc_b200_extract_paths     <- _trace_path + cost, cuda-rrtc/jax/prrtc.py:556-640
+ *   prrtc_b200_result_block      <- the device_get of every output and the per-result loop,
+ *                                   cuda-rrtc/jax/prrtc.py:1399-1434
+ *                                   (sizes, flags, paths): one block and one path copy
  *   prrtc_b200_check_configs     <- the collision checkers, prrtc_planner.cu:234-655
  *                                   (exposed as a batched primitive)
  *   prrtc_b200_fk / _halton      <- fk_single call sites (prrtc_planner.cu:509-522) and the
@@ -346,6 +349,22 @@ int prrtc_b200_extract_paths(int32_t batch, int32_t dim, int32_t max_nodes,
                              const int32_t* connection_info, const int32_t* solved_flag,
                              int32_t max_len, float* paths, int32_t* lengths, float* costs,
                              void* stream);
+
+/* The scalars of B planner results gathered into one int32 block [B,16] for a
+ * single device->host copy: columns 0-1 tree sizes, 2-3 completed flags, 4
+ * iterations, 5-7 connection_info, 8 solved_flag, 9 kernel_ms (float bits), 10
+ * path length and 11 path cost (float bits, from prrtc_b200_extract_paths), 12
+ * the path's first waypoint in packed_paths or -1, 13-15 zero.  With packed_paths
+ * (capacity packed_capacity waypoints of dim floats), the solved paths of
+ * paths [B,max_len,dim] are also copied back to back, in problem order, into
+ * packed_paths; a path past the capacity gets -1 in column 12 and stays only in
+ * paths.  packed_paths may be NULL (block only). */
+int prrtc_b200_result_block(int32_t batch, int32_t dim, int32_t max_len,
+                            const int32_t* sizes, const int32_t* completed, const int32_t* iterations,
+                            const int32_t* connection_info, const int32_t* solved_flag,
+                            const float* kernel_ms, const int32_t* lengths, const float* costs,
+                            const float* paths, int32_t* block, float* packed_paths,
+                            int64_t packed_capacity, void* stream);
 
 /* Smooth collision + length cost of P paths of W waypoints [P,W,dim] and its
  * gradient (hand-written adjoint through FK, link transforms recomputed):

@@ -100,7 +100,7 @@ EXPORTS = (
     "prrtc_b200_iteration",
     "prrtc_b200_point_cloud_workspace_size", "prrtc_b200_point_cloud_build",
     "prrtc_b200_check_edges_workspace_size", "prrtc_b200_check_edges",
-    "prrtc_b200_fk", "prrtc_b200_halton", "prrtc_b200_extract_paths",
+    "prrtc_b200_fk", "prrtc_b200_halton", "prrtc_b200_extract_paths", "prrtc_b200_result_block",
     "prrtc_b200_smooth_workspace_size", "prrtc_b200_smooth_cost_grad",
     "prrtc_b200_smooth_batch_workspace_size", "prrtc_b200_smooth_cost_grad_batch",
     "prrtc_b200_choose_tree", "prrtc_b200_radius_update",
@@ -126,6 +126,7 @@ _SIGS = {
     "prrtc_b200_fk": (C.c_int, [P, I32, P, I32, P, P]),
     "prrtc_b200_halton": (C.c_int, [I32, I32, I32, P, P, P, P]),
     "prrtc_b200_extract_paths": (C.c_int, [I32, I32, I32, P, P, P, P, P, P, I32, P, P, P, P]),
+    "prrtc_b200_result_block": (C.c_int, [I32, I32, I32, P, P, P, P, P, P, P, P, P, P, P, C.c_int64, P]),
     "prrtc_b200_smooth_workspace_size": (C.c_size_t, [P, P]),
     "prrtc_b200_smooth_cost_grad": (C.c_int, [P, P, I32, P, I32, I32, F32, F32, F32, P, P, P, C.c_size_t, P]),
     "prrtc_b200_smooth_batch_workspace_size": (C.c_size_t, [P]),

@@ -472,6 +472,22 @@ int prrtc_b200_extract_paths(int32_t batch, int32_t dim, int32_t max_nodes, cons
     return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
 }
 
+int prrtc_b200_result_block(int32_t batch, int32_t dim, int32_t max_len, const int32_t* sizes,
+                            const int32_t* completed, const int32_t* iterations, const int32_t* connection_info,
+                            const int32_t* solved_flag, const float* kernel_ms, const int32_t* lengths,
+                            const float* costs, const float* paths, int32_t* block, float* packed_paths,
+                            int64_t packed_capacity, void* stream) {
+    if (batch == 0) return PRRTC_B200_OK;
+    if (batch < 0 || !sizes || !completed || !iterations || !connection_info || !solved_flag || !kernel_ms ||
+        !lengths || !costs || !block || packed_capacity < 0 || (packed_paths && (!paths || max_len < 1)))
+        return PRRTC_B200_EARG;
+    if (dim < 1 || dim > PRRTC_B200_DIM_MAX) return PRRTC_B200_EUNSUPPORTED;
+    const ResultSrc R{sizes, completed, iterations, connection_info, solved_flag, kernel_ms, lengths, costs};
+    cudaError_t e = launch_result_block(batch, dim, max_len, R, block, paths, packed_paths, packed_capacity,
+                                        static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? PRRTC_B200_OK : cuda_fail(e);
+}
+
 size_t prrtc_b200_smooth_workspace_size(const prrtc_robot_t* robot, const prrtc_world_t* world) {
     if (!robot || !world) return 0;
     return blob_stride(make_pack(*robot, *world, 1, 0, 0.0f));

@@ -85,6 +85,26 @@ cudaError_t launch_extract_paths(int B, int dim, int N, const float* ta, const f
                                  const int32_t* pb, const int32_t* conn, const int32_t* solved, int max_len,
                                  float* paths, int32_t* lengths, float* costs, cudaStream_t st);
 
+// Columns of the [B,16] int32 result block.
+enum : int {
+    kBlkSizeA = 0, kBlkSizeB = 1, kBlkCompletedA = 2, kBlkCompletedB = 3, kBlkIterations = 4, kBlkConn = 5,
+    kBlkSolved = 8, kBlkKernelMs = 9, kBlkLength = 10, kBlkCost = 11, kBlkOffset = 12
+};
+
+// Per-problem planner outputs that the result block gathers.
+struct ResultSrc {
+    const int32_t* sizes;      // [B,2]
+    const int32_t* completed;  // [B,2]
+    const int32_t* iterations; // [B]
+    const int32_t* conn;       // [B,3]
+    const int32_t* solved;     // [B]
+    const float* kernel_ms;    // [B]
+    const int32_t* lengths;    // [B]
+    const float* costs;        // [B]
+};
+cudaError_t launch_result_block(int B, int dim, int max_len, const ResultSrc& R, int32_t* block,
+                                const float* paths, float* packed, long long packed_cap, cudaStream_t st);
+
 // primitives.cu
 cudaError_t launch_nearest(const float* tree, int dim, int N, const int32_t* tree_size, const float* q, int batch,
                            int32_t* idx, float* dist, unsigned long long* keys, cudaStream_t st);

@@ -934,4 +934,85 @@ cudaError_t launch_extract_paths(int B, int dim, int N, const float* ta, const f
     return cudaGetLastError();
 }
 
+// Result block: one [B,16] int32 row per problem (columns kBlk*), the scalars
+// a caller reads back in one copy.  Column kBlkOffset is the exclusive prefix
+// sum of the solved path lengths (one CTA, chunks of 1024 problems scanned
+// with warp shuffles), or -1 for a problem whose path is not packed: unsolved,
+// longer than the path buffer, or past packed_cap waypoints.
+__global__ void result_block_kernel(int B, const ResultSrc R, int32_t* block, long long packed_cap) {
+    __shared__ long long warp_sum[32];
+    __shared__ long long s_carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_carry = 0;
+    __syncthreads();
+    for (int b0 = 0; b0 < B; b0 += blockDim.x) {
+        const int b = b0 + tid;
+        int len = 0;
+        if (b < B) len = (R.solved[b] == 1 && R.lengths[b] > 0) ? R.lengths[b] : 0;
+        long long x = len;  // inclusive scan within the warp
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) warp_sum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            const int nwarps = blockDim.x >> 5;
+            long long v = lane < nwarps ? warp_sum[lane] : 0;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, v, off);
+                if (lane >= off) v += y;
+            }
+            if (lane < nwarps) warp_sum[lane] = v;  // inclusive over warps
+        }
+        __syncthreads();
+        const long long carry = s_carry;
+        const long long excl = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - len;
+        if (b < B) {
+            int32_t* row = block + (size_t)b * 16;
+            row[kBlkSizeA] = R.sizes[2 * b];
+            row[kBlkSizeB] = R.sizes[2 * b + 1];
+            row[kBlkCompletedA] = R.completed[2 * b];
+            row[kBlkCompletedB] = R.completed[2 * b + 1];
+            row[kBlkIterations] = R.iterations[b];
+            row[kBlkConn + 0] = R.conn[3 * b];
+            row[kBlkConn + 1] = R.conn[3 * b + 1];
+            row[kBlkConn + 2] = R.conn[3 * b + 2];
+            row[kBlkSolved] = R.solved[b];
+            row[kBlkKernelMs] = __float_as_int(R.kernel_ms[b]);
+            row[kBlkLength] = R.lengths[b];
+            row[kBlkCost] = __float_as_int(R.costs[b]);
+            row[kBlkOffset] = (len > 0 && excl + len <= packed_cap) ? (int32_t)excl : -1;
+            row[13] = row[14] = row[15] = 0;
+        }
+        __syncthreads();
+        if (tid == blockDim.x - 1) s_carry = carry + warp_sum[(blockDim.x >> 5) - 1];
+        __syncthreads();
+    }
+}
+
+// Solved paths copied back to back into packed (the offsets of the result
+// block), so that a caller reads every path with one contiguous copy.
+__global__ void pack_paths_kernel(int B, int dim, int max_len, const float* paths, const int32_t* block,
+                                  float* packed) {
+    const int b = blockIdx.x;
+    const int32_t* row = block + (size_t)b * 16;
+    const int off = row[kBlkOffset], len = row[kBlkLength];
+    if (off < 0 || len <= 0) return;
+    const float* src = paths + (size_t)b * max_len * dim;
+    float* dst = packed + (size_t)off * dim;
+    for (int i = threadIdx.x; i < len * dim; i += blockDim.x) dst[i] = src[i];
+}
+
+cudaError_t launch_result_block(int B, int dim, int max_len, const ResultSrc& R, int32_t* block,
+                                const float* paths, float* packed, long long packed_cap, cudaStream_t st) {
+    result_block_kernel<<<1, 1024, 0, st>>>(B, R, block, packed ? packed_cap : 0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !packed || packed_cap <= 0) return e;
+    pack_paths_kernel<<<B, 64, 0, st>>>(B, dim, max_len, paths, block, packed);
+    return cudaGetLastError();
+}
+
 }  // namespace prrtc

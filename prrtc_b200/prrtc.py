@@ -40,6 +40,16 @@ from .device import REQUIRED_KEYS, DeviceContext, Stager, as_tensor, cuda_device
 
 _COLLISION_MODES = {"binary": 0, "differentiable": 1, "binary_coarse": 2, "binary_coarse_coop": 3}
 PATH_MAX_LEN = 16384
+_SIDE_STREAMS: dict = {}
+
+
+def _side_stream(device: torch.device) -> torch.cuda.Stream:
+    """A stream of this module's own per device, for read-backs that must wait
+    for one call only and not for later work queued on the caller's stream."""
+    key = device.index if device.index is not None else torch.cuda.current_device()
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = torch.cuda.Stream(device=device)
+    return _SIDE_STREAMS[key]
 
 
 class PRRTCResult(NamedTuple):
@@ -161,38 +171,90 @@ class _Results:
         self.paths = torch.empty((B, self.max_len, dim), dtype=torch.float32, device=device)
         self.lengths = torch.empty((B,), dtype=torch.int32, device=device)
         self.costs = torch.empty((B,), dtype=torch.float32, device=device)
+        self.packed = self.packed_h = self.block_h = self.ready = None
+        self.d2h_bytes = 0  # device->host bytes of the read-back
 
     def outputs(self) -> _lib.Outputs:
         return _outputs_struct(self.ta, self.tb, self.pa, self.pb, self.sizes, self.completed, self.iters,
                                self.conn, self.solved, self.ktime)
 
-    def extract(self, stream_ptr: int) -> None:
+    def extract(self, stream_ptr: int, pack_paths: bool = False) -> None:
+        """Queue path extraction and the result block; with ``pack_paths`` the
+        solved paths are also copied back to back into ``self.packed`` (the
+        block's column 12 holds each path's first row there)."""
         lib = _lib.load()
         _lib.check(lib.prrtc_b200_extract_paths(self.B, self.dim, self.N, ptr(self.ta), ptr(self.tb), ptr(self.pa),
                                                 ptr(self.pb), ptr(self.conn), ptr(self.solved), self.max_len,
                                                 ptr(self.paths), ptr(self.lengths), ptr(self.costs), stream_ptr),
                    "prrtc_b200_extract_paths")
-        b = self.block
-        b[:, 0:2] = self.sizes
-        b[:, 2:4] = self.completed
-        b[:, 4:5] = self.iters
-        b[:, 5:8] = self.conn
-        b[:, 8:9] = self.solved
-        b[:, 9] = self.ktime.view(torch.int32)
-        b[:, 10] = self.lengths
-        b[:, 11] = self.costs.view(torch.int32)
+        # room for an average of 128 waypoints per path (at least 65536 in all);
+        # a path past it is read from the path buffer on its own
+        rows = min(self.B * self.max_len, max(128 * self.B, 65536))
+        self.packed = (torch.empty((rows, self.dim), dtype=torch.float32, device=self.paths.device)
+                       if pack_paths else None)
+        _lib.check(lib.prrtc_b200_result_block(
+            self.B, self.dim, self.max_len, ptr(self.sizes), ptr(self.completed), ptr(self.iters), ptr(self.conn),
+            ptr(self.solved), ptr(self.ktime), ptr(self.lengths), ptr(self.costs), ptr(self.paths), ptr(self.block),
+            ptr(self.packed), 0 if self.packed is None else self.packed.shape[0], stream_ptr),
+            "prrtc_b200_result_block")
+
+    def prefetch_host(self, path_rows: int = 0) -> None:
+        """Queue, on the current stream right behind the planner's kernels, the
+        device->host copies that ``to_results`` needs: the result block and the
+        first ``path_rows`` rows of the packed paths, into pinned memory, then an
+        event.  Copies issued this way run on the copy engine as soon as this
+        call's kernels are done; a copy issued later, when the stream or the
+        GPU already holds the next call's persistent planner, would wait for it."""
+        self.block_h = torch.empty((self.B, 16), dtype=torch.int32, pin_memory=True)
+        self.block_h.copy_(self.block, non_blocking=True)
+        self.d2h_bytes = self.block.numel() * 4
+        self.packed_h = None
+        if self.packed is not None and path_rows > 0:
+            n = min(int(path_rows), self.packed.shape[0])
+            self.packed_h = torch.empty((n, self.dim), dtype=torch.float32, pin_memory=True)
+            self.packed_h.copy_(self.packed[:n], non_blocking=True)
+            self.d2h_bytes += self.packed_h.numel() * 4
+        self.ready = torch.cuda.Event()
+        self.ready.record()
+
+    def _host_paths(self, host: np.ndarray) -> Optional[np.ndarray]:
+        """Every solved path on the host: rows of the packed paths (prefetched,
+        plus the rest copied now on a side stream that waits only for this
+        call), or the [B, longest] slice of the path buffer."""
+        if self.packed is None:
+            lmax = int(max(0, host[:, 10].max())) if self.B else 0
+            return self.paths[:, :lmax].cpu().numpy() if lmax > 0 else None
+        ok = host[:, 12] >= 0
+        total = int((host[ok, 12] + host[ok, 10]).max()) if ok.any() else 0
+        if self.ready is None:  # nothing prefetched: read on the caller's stream
+            return self.packed[:total].cpu().numpy() if total else None
+        have = 0 if self.packed_h is None else self.packed_h.shape[0]
+        parts = [self.packed_h.numpy()[:min(have, total)]] if have else []
+        if total > have:
+            side = _side_stream(self.packed.device)
+            side.wait_event(self.ready)
+            with torch.cuda.stream(side):
+                rest = torch.empty((total - have, self.dim), dtype=torch.float32, pin_memory=True)
+                rest.copy_(self.packed[have:total], non_blocking=True)
+            self.d2h_bytes += rest.numel() * 4
+            side.synchronize()
+            parts.append(rest.numpy())
+        # a private copy: the pinned blocks go back to the allocator's cache now
+        return np.concatenate(parts, 0) if len(parts) > 1 else (parts[0].copy() if parts else None)
 
     def to_results(self, trees: bool = True, paths_on_host: bool = False) -> list[PRRTCResult]:
         """One read-back of the [B,16] scalar block (plus, with paths_on_host, one
         bulk copy of every path) and the per-problem PRRTCResults."""
-        host = self.block.cpu().numpy()
+        if self.ready is not None:
+            self.ready.synchronize()
+            host = self.block_h.numpy().copy()
+        else:
+            host = self.block.cpu().numpy()
         if (host[:, 8] == -2).any():
             raise _lib.PrrtcError("a device-side wait ran out (scene staging): the planner stopped and these "
                                   "results are incomplete")
-        hpaths = None
-        if paths_on_host:
-            lmax = int(max(0, host[:, 10].max())) if self.B else 0
-            hpaths = self.paths[:, :lmax].cpu().numpy() if lmax > 0 else None
+        hpaths = self._host_paths(host) if paths_on_host else None
+        packed = self.packed is not None and paths_on_host
         out = []
         # plain Python scalars for the per-problem loop (numpy scalar access is slow)
         rows = host.tolist()
@@ -209,7 +271,10 @@ class _Results:
             cost = costs[i] if solved else inf
             path = None
             if solved:
-                if length > 0:
+                if length > 0 and packed:
+                    path = (from_numpy(hpaths[row[12]:row[12] + length]) if row[12] >= 0
+                            else self._path_row(i, length))  # past the packed capacity
+                elif length > 0:
                     path = from_numpy(hpaths[i, :length]) if hpaths is not None else self.paths[i, :length]
                 else:  # longer than the device path buffer: walk on the host
                     path = self._host_trace(i)
@@ -227,6 +292,19 @@ class _Results:
                 tbp = (self.pb[i] if batched else self.pb)[:nb]
             # field order of PRRTCResult
             out.append(make(PRRTCResult, (solved, path, size_a, size_b, row[4], cost, kts[i], tac, tbc, tap, tbp)))
+        return out
+
+    def _path_row(self, i: int, length: int) -> torch.Tensor:
+        """Path i from the path buffer to the host, on the side stream (waits for
+        this call only)."""
+        if self.ready is None:
+            return self.paths[i, :length].cpu()
+        side = _side_stream(self.paths.device)
+        side.wait_event(self.ready)
+        with torch.cuda.stream(side):
+            out = self.paths[i, :length].to("cpu", non_blocking=True)
+        side.synchronize()
+        self.d2h_bytes += out.numel() * 4
         return out
 
     def _host_trace(self, i: int) -> torch.Tensor:
@@ -505,8 +583,14 @@ def prrtc_plan_batch_async(
 ) -> "PendingBatch":
     """Plan B independent problems (prrtc.py:882-1434), without waiting: the
     work is queued on the current stream and ``.results()`` of the returned
-    handle reads it back.  Several batches (for example one per tree-capacity
-    bucket, each on its own stream) can be in flight at once.
+    handle reads it back.  Several batches can be in flight at once; queue
+    back-to-back batches on ONE stream.  The persistent planner holds every SM
+    until its batch is done, so a planner launch queued on a second stream
+    takes the SMs that the first batch's tail frees, and the first batch's
+    closing kernels (finalize, path extraction) then wait for the whole second
+    batch.  Each call queues its device->host read-back right behind its own
+    kernels, so ``.results()`` of an earlier call waits for that call only,
+    not for later calls on the same stream.
 
     ``collision_context`` is one dict shared by every problem, or a list/tuple of
     per-problem dicts (robot tables from the first non-None entry; worlds and
@@ -664,7 +748,10 @@ def prrtc_plan_batch_async(
         _plan_per_problem(lib, bi, res, attrs, tun, contexts, robot_ctx, starts, goals, goal_counts, lo, hi, dev)
     else:
         raise ValueError(f"launch must be 'persistent' or 'per_problem', got {launch!r}")
-    res.extract(sp)
+    res.extract(sp, pack_paths=paths_on_host)
+    # the read-back is queued now, behind this call's kernels (about 24 waypoints
+    # per path prefetched; longer paths cost one more copy in results())
+    res.prefetch_host(24 * B if paths_on_host else 0)
     # everything the queued kernels read stays referenced until results()
     keep += [robot_ctx] + ([ws] if launch == "persistent" else [])
     return PendingBatch(res, keep, torch.cuda.current_stream(dev), return_trees, paths_on_host)
@@ -682,6 +769,11 @@ class PendingBatch:
             out = self.res.to_results(trees=self.trees, paths_on_host=self.paths_on_host)
         self.keep = []
         return out
+
+    @property
+    def d2h_bytes(self) -> int:
+        """Bytes read back to the host by the prefetch and ``results()``."""
+        return self.res.d2h_bytes
 
 
 def prrtc_plan_batch(start_configs, goal_configs, *args, **kwargs) -> list[PRRTCResult]:

@@ -436,6 +436,90 @@ def test_async_batches_on_two_streams(cuda, orc):
                 assert ok, md
 
 
+def test_async_batches_pipelined_on_one_stream(cuda, orc):
+    """Three calls queued on one stream before the first is read back (the
+    bench's end-to-end form): every call's results, read in order, match its own
+    problems, and every packed path re-validates."""
+    from prrtc_b200 import prrtc_plan_batch_async
+
+    batches = [[make_problem("uneven", 420 + 10 * k + i) for i in range(5)] for k in range(3)]
+    st = torch.cuda.Stream(device=cuda)
+    pending = []
+    with torch.cuda.stream(st):
+        for probs in batches:
+            G = max(p.goals.shape[0] for p in probs)
+            goals = np.zeros((len(probs), G, probs[0].dim), np.float32)
+            for i, p in enumerate(probs):
+                goals[i, : p.goals.shape[0]] = p.goals
+            pending.append(prrtc_plan_batch_async(
+                np.stack([p.start for p in probs]), goals, max_iterations=5000, num_new_samples=4,
+                max_nodes=[p.max_nodes for p in probs], min_vals=probs[0].lower, max_vals=probs[0].upper,
+                collision_context=[p.context for p in probs], collision_checker="binary_coarse_coop",
+                goal_counts=[p.goals.shape[0] for p in probs], edge_resolution=0.01, return_trees=False,
+                paths_on_host=True))
+    for probs, pend in zip(batches, pending):
+        res = pend.results()
+        assert pend.d2h_bytes >= len(probs) * 64
+        assert sum(r.solved for r in res) >= len(probs) - 1
+        for p, r in zip(probs, res):
+            if r.solved:
+                path = r.path.numpy()
+                assert path.shape[1] == p.dim and r.path.device.type == "cpu"
+                assert np.array_equal(path[0], p.start.astype(np.float32))
+                assert any(np.array_equal(path[-1], g.astype(np.float32)) for g in p.goals)
+                ok, md = orc.Scene(p.context, p.dim).validate_path(path, 0.01)
+                assert ok, md
+                assert abs(r.cost - np.linalg.norm(np.diff(path, axis=0), axis=1).sum()) < 1e-3 * max(1.0, r.cost)
+
+
+def test_result_block_and_packed_paths(cuda):
+    """prrtc_b200_result_block through the C-ABI against a numpy restatement:
+    1500 problems (two chunks of the one-CTA scan), unsolved, failed, empty and
+    too-long (-1) paths, and a packed capacity that the last paths overflow."""
+    from prrtc_b200 import _lib
+
+    lib = _lib.load()
+    rng = np.random.default_rng(5)
+    B, dim, L = 1500, 7, 40
+    solved = rng.choice([1, 1, 1, 0, -1], B).astype(np.int32)
+    lengths = rng.integers(1, L + 1, B).astype(np.int32)
+    lengths[rng.random(B) < 0.05] = -1
+    lengths[solved != 1] = 0
+    sizes = rng.integers(1, 1 << 20, (B, 2)).astype(np.int32)
+    completed = rng.integers(0, 2, (B, 2)).astype(np.int32)
+    iters = rng.integers(0, 10000, B).astype(np.int32)
+    conn = rng.integers(-1, 1000, (B, 3)).astype(np.int32)
+    kms = rng.random(B).astype(np.float32)
+    costs = rng.random(B).astype(np.float32)
+    paths = rng.standard_normal((B, L, dim)).astype(np.float32)
+    live = (solved == 1) & (lengths > 0)
+    cap = int(lengths[live].sum()) - 500  # the last few paths do not fit
+    t = {k: torch.from_numpy(v).to(cuda) for k, v in dict(sizes=sizes, completed=completed, iters=iters, conn=conn,
+                                                          solved=solved, kms=kms, lengths=lengths, costs=costs,
+                                                          paths=paths).items()}
+    block = torch.full((B, 16), 77, dtype=torch.int32, device=cuda)
+    packed = torch.full((cap, dim), np.nan, dtype=torch.float32, device=cuda)
+    rc = lib.prrtc_b200_result_block(B, dim, L, *(t[k].data_ptr() for k in ("sizes", "completed", "iters", "conn",
+                                                                         "solved", "kms", "lengths", "costs",
+                                                                         "paths")),
+                                     block.data_ptr(), packed.data_ptr(), cap, torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    got = block.cpu().numpy()
+    off = np.concatenate([[0], np.cumsum(np.where(live, lengths, 0))[:-1]])
+    want_off = np.where(live & (off + np.where(live, lengths, 0) <= cap), off, -1)
+    want = np.zeros((B, 16), np.int32)
+    want[:, 0:2], want[:, 2:4], want[:, 4], want[:, 5:8] = sizes, completed, iters, conn
+    want[:, 8], want[:, 9], want[:, 10], want[:, 11], want[:, 12] = solved, kms.view(np.int32), lengths, \
+        costs.view(np.int32), want_off
+    assert np.array_equal(got, want)
+    assert (want_off == -1).sum() > (~live).sum()  # some live paths overflowed
+    pk = packed.cpu().numpy()
+    for b in np.flatnonzero(want_off >= 0):
+        assert np.array_equal(pk[want_off[b]:want_off[b] + lengths[b]], paths[b, :lengths[b]])
+    used = int((want_off + lengths)[want_off >= 0].max())
+    assert np.isnan(pk[used:]).all()  # nothing written past the last packed path
+
+
 def test_staging_wait_that_runs_out_reports_minus_two(cuda):
     """Failure path of the bounded scene-staging wait, without a fault: with no
     polls allowed every CTA's wait gives up at once (its copy still lands
