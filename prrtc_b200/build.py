@@ -54,14 +54,16 @@ def up_to_date() -> bool:
 
 
 def build_hostpack(force: bool = False) -> Path:
-    """g++ -O2 -shared of the CPython host packer."""
+    """g++ -O2 -shared of the CPython host packer (CPython and numpy C APIs)."""
     if not force and HOSTPACK.exists() and all(
             p.stat().st_mtime <= HOSTPACK.stat().st_mtime for p in (HOSTPACK_SRC, Path(__file__))):
         return HOSTPACK
     cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
     tmp = HOSTPACK.with_name(HOSTPACK.name + ".tmp")
+    import numpy
+
     cmd = [cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fno-strict-aliasing", "-Wall",
-           "-I", sysconfig.get_paths()["include"], str(HOSTPACK_SRC), "-o", str(tmp)]
+           "-I", sysconfig.get_paths()["include"], "-I", numpy.get_include(), str(HOSTPACK_SRC), "-o", str(tmp)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"g++ failed for {HOSTPACK_SRC.name}:\n{r.stdout}\n{r.stderr}")

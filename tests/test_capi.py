@@ -193,10 +193,32 @@ def test_native_host_packer_declines_other_types():
                 np.zeros((2, 5), np.float32), np.zeros(8, np.float32)):
         with pytest.raises(TypeError):
             hp.scan([good, {"world_spheres": bad}], _PACK_SPECS)
+    with pytest.raises(TypeError):
+        hp.scan([good, {"self_pairs": np.zeros((2, 2), np.int64)}], _PACK_SPECS)
     info = hp.scan([good, good], _PACK_SPECS)
     layout, total = _native_layout(info, _PACK_SPECS, 2)
     with pytest.raises(ValueError):
         hp.fill([good, good], _PACK_SPECS, layout, np.zeros(max(total - 1, 0), np.uint8))
+
+
+def test_native_host_packer_reads_non_numpy_buffers():
+    """A table that is not a numpy array but exports a C-contiguous float32
+    buffer (a memoryview here) is read through the buffer protocol: same scan
+    and same bytes as the numpy array."""
+    from prrtc_b200 import _lib
+    from prrtc_b200.prrtc import _PACK_SPECS
+
+    hp = _lib.hostpack()
+    a = np.arange(12, dtype=np.float32).reshape(3, 4)
+    ctxs_np = [{"world_spheres": a}, {"world_spheres": a[:1].copy()}]
+    ctxs_mv = [{"world_spheres": memoryview(a)}, {"world_spheres": memoryview(a[:1].copy())}]
+    info_np, info_mv = hp.scan(ctxs_np, _PACK_SPECS), hp.scan(ctxs_mv, _PACK_SPECS)
+    assert info_np == info_mv
+    layout, total = _native_layout(info_np, _PACK_SPECS, 2)
+    b1, b2 = np.zeros(total, np.uint8), np.zeros(total, np.uint8)
+    hp.fill(ctxs_np, _PACK_SPECS, layout, b1)
+    hp.fill(ctxs_mv, _PACK_SPECS, layout, b2)
+    assert np.array_equal(b1, b2) and b1.any()
 
 
 def test_autotuner_second_round_decides(monkeypatch):
