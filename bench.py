@@ -453,7 +453,8 @@ def run_ours(a):
     if not a.no_extras:
         if ws > 1:
             dist.barrier()
-        e_solved, e_s, e_h2d, e_d2h, e_steps = measure_e2e(torch, dev, planners, settings, tuned, cap_of, a.steps)
+        e_solved, e_s, e_h2d, e_d2h, e_steps, e_diag = measure_e2e(torch, dev, planners, settings, tuned, cap_of,
+                                                                    a.steps)
         if ws > 1:
             v = torch.tensor([e_s, float(e_solved), float(e_h2d), float(e_d2h)], dtype=torch.float64, device=dev)
             vmax = v[:1].clone()
@@ -462,7 +463,7 @@ def run_ours(a):
             dist.all_reduce(vsum, op=dist.ReduceOp.SUM)
             e_s, e_solved, e_h2d, e_d2h = float(vmax.item()), *(float(x) for x in vsum.tolist())
         line["e2e"] = {"value": e_solved / e_s, "unit": "plans/s", "h2d_bytes_per_step": int(e_h2d),
-                       "d2h_bytes_per_step": int(e_d2h), "steps": e_steps,
+                       "d2h_bytes_per_step": int(e_d2h), "steps": e_steps, "rank0_timed_region": e_diag,
                        "api": "prrtc_b200.prrtc_plan_batch_async + .results() (per-problem collision_context "
                               "dicts, host numpy inputs, one call per step for all of a rank's problems, up to "
                               "three steps in flight on one stream: later steps are packed and copied while "
@@ -675,27 +676,49 @@ def measure_e2e(torch, dev, planners, settings, tuned, cap_of, steps):
             d2h += pend.d2h_bytes
         return solved, d2h
 
-    # warm in the timed form (depth calls in flight), so that the caching
-    # allocators already hold the device and pinned blocks of three concurrent
-    # calls: a cudaMalloc / cudaHostAlloc inside the timed region costs ms
-    warm = [enqueue(k) for k in range(depth)]
-    for pending in warm:
-        collect(pending)
+    def pipeline(n, marks=None):
+        """n steps, depth calls in flight; returns (plans solved, d2h bytes)."""
+        solved = d2h = 0
+        inflight = [enqueue(k) for k in range(min(depth - 1, n))]
+        for k in range(n):
+            if k + depth - 1 < n:
+                inflight.append(enqueue(k + depth - 1))
+            s_, d_ = collect(inflight.pop(0))
+            solved += s_
+            d2h += d_
+            if marks is not None:
+                marks.append(time.perf_counter())
+        return solved, d2h
+
+    # warm with the timed loop itself, so that the caching allocators already
+    # hold every device and pinned block its allocation pattern needs: a
+    # cudaMalloc / cudaHostAlloc inside the timed region costs milliseconds
+    pipeline(2 * depth + 2)
     torch.cuda.synchronize()
     _device.H2D_BYTES[0] = 0
     k_e2e = max(1, int(steps))
-    solved = d2h = 0
+    # diagnostics of the timed region: host time per step, device allocations
+    # (cudaMalloc by the caching allocator) and garbage-collector pauses
+    gc_ms = [0.0, 0.0]
+
+    def gc_cb(phase, info):
+        if phase == "start":
+            gc_ms[1] = time.perf_counter()
+        else:
+            gc_ms[0] += (time.perf_counter() - gc_ms[1]) * 1e3
+    gc.callbacks.append(gc_cb)
+    allocs0 = torch.cuda.memory_stats(dev).get("num_device_alloc", 0)
+    marks = []
     t0 = time.perf_counter()
-    inflight = [enqueue(k) for k in range(min(depth - 1, k_e2e))]
-    for k in range(k_e2e):
-        if k + depth - 1 < k_e2e:
-            inflight.append(enqueue(k + depth - 1))
-        s_, d_ = collect(inflight.pop(0))
-        solved += s_
-        d2h += d_
+    solved, d2h = pipeline(k_e2e, marks)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    return solved, dt, _device.H2D_BYTES[0] // k_e2e, d2h // k_e2e, k_e2e
+    gc.callbacks.remove(gc_cb)
+    step_ms = np.diff(np.asarray([t0] + marks)) * 1e3
+    diag = {"step_ms_p50": float(np.median(step_ms)), "step_ms_max": float(step_ms.max()),
+            "first_step_ms": float(step_ms[0]), "gc_ms": gc_ms[0],
+            "device_allocs": int(torch.cuda.memory_stats(dev).get("num_device_alloc", 0) - allocs0)}
+    return solved, dt, _device.H2D_BYTES[0] // k_e2e, d2h // k_e2e, k_e2e, diag
 
 
 def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
