@@ -775,8 +775,6 @@ struct CcBufs {
 };
 
 constexpr int kMaxParts = 256;  // world parts per chunk (cost-balanced obstacle ranges)
-constexpr int kGroupW = 8;      // edge waypoints per coarse group bound
-constexpr float kGroupSlack = 1.0e-5f;  // metres added to a group bound (float error of the distance tests)
 
 __host__ __device__ inline int cc_smem_bytes(int J, int S, int K, int Q, int CW) {
     const int S_pad = odd_pad(S);
@@ -893,22 +891,10 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     const int n_parts = n_obs == 0 ? 0
                         : full_sweep ? min(kMaxParts, max(1, min(T / max(1, nw * h.n_sch), cdiv(n_obs, 4))))
                                      : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * h.n_sch)), cdiv(n_obs, 4))));
-    // coarse pass: one item = up to 8 coarse spheres of a unit over a part.  A unit
-    // is one waypoint, or, for the waypoints of an edge (consecutive configurations
-    // a resolution step apart), a group of kGroupW of them: each coarse sphere is
-    // then first tested as one sphere bounding its kGroupW positions, and a hit
-    // marks the sphere dirty at every waypoint of the group.  The fine pass decides
-    // every verdict, so the verdicts are those of the per-waypoint gate; the
-    // bound only lets most of the coarse tests go (a link's bound over 8
-    // waypoints of a 0.01 rad step is dirty about as often as the link itself).
+    // coarse pass: one item = up to 8 coarse spheres of a waypoint over a part
     const int KC = cdiv(K, 8);
-    const int n_grp = cdiv(nw, kGroupW);
-    const bool grouped = gated && edge_mode && nw > kGroupW && n_grp * K * 4 <= B.listcap / 2;
-    const int n_units = grouped ? n_grp : nw;
-    const int listcap = grouped ? B.listcap - n_grp * K * 4 : B.listcap;
-    float4* gsph = reinterpret_cast<float4*>(B.pose + listcap);  // [n_grp][K] group bounds (grouped only)
     const int n_parts_c =
-        (n_obs == 0 || !gated) ? 0 : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, n_units * KC)), cdiv(n_obs, 4))));
+        (n_obs == 0 || !gated) ? 0 : min(kMaxParts, max(1, min(cdiv(2 * T, max(1, nw * KC)), cdiv(n_obs, 4))));
     int* bounds_c = B.bounds + (kMaxParts + 1);
     if (n_parts > 0)
         for (int i = tid; i <= n_parts; i += T) B.bounds[i] = world_index_at(h, (int)((long long)i * ctot / n_parts));
@@ -987,53 +973,22 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
         B.hit[par] = 0u;  // par was flipped: this is the word the next call uses
         B.hit[2] = B.hit[3] = 0u;  // work-list counters
     }
-    if (grouped) {
-        // bound of coarse sphere k over the waypoints of group gi: centre of the
-        // box around the centres, radius the largest distance to a centre plus the
-        // sphere's radius, rounded up so that float error never makes it smaller
-        // than a per-waypoint sphere (absent spheres stay NaN)
-        for (int i = tid; i < n_grp * K; i += T) {
-            const int gi = i / K, k = i - gi * K;
-            const int w0 = gi * kGroupW, w1 = min(nw, w0 + kGroupW);
-            const float4 c0 = B.cctr[w0 * K + k];
-            float lx = c0.x, ly = c0.y, lz = c0.z, hx = c0.x, hy = c0.y, hz = c0.z;
-            for (int w = w0 + 1; w < w1; ++w) {
-                const float4 c = B.cctr[w * K + k];
-                lx = fminf(lx, c.x); ly = fminf(ly, c.y); lz = fminf(lz, c.z);
-                hx = fmaxf(hx, c.x); hy = fmaxf(hy, c.y); hz = fmaxf(hz, c.z);
-            }
-            const float mx = 0.5f * (lx + hx), my = 0.5f * (ly + hy), mz = 0.5f * (lz + hz);
-            float d2 = 0.0f;
-            for (int w = w0; w < w1; ++w) {
-                const float4 c = B.cctr[w * K + k];
-                const float dx = c.x - mx, dy = c.y - my, dz = c.z - mz;
-                d2 = fmaxf(d2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-            }
-            const float r = (sqrtf(d2) + c0.w) * (1.0f + 1.0e-6f) + kGroupSlack;
-            gsph[i] = (c0.x == c0.x) ? make_float4(mx, my, mz, r) : absent_sphere();
-        }
-        g.sync();
-    }
     unsigned long long flops = 0;
     // D: coarse pre-pass -> dirty groups and touching coarse self pairs
     if (gated) {
-        const int n_cw = n_units * KC * n_parts_c;
+        const int n_cw = nw * KC * n_parts_c;
         for (int it = tid; it < n_cw + nw * Q; it += T) {
             if (it < n_cw) {
-                const int part = it / (n_units * KC), r = it - part * (n_units * KC);
-                const int kc = r / n_units, u = r - kc * n_units;
+                const int part = it / (nw * KC), r = it - part * (nw * KC);
+                const int kc = r / nw, w = r - kc * nw;
                 const int k0 = kc * 8, nk = min(8, K - k0);
-                const float4* src = grouped ? gsph : B.cctr;
                 float4 s[8];
 #pragma unroll
-                for (int m = 0; m < 8; ++m) s[m] = m < nk ? src[u * K + k0 + m] : absent_sphere();
+                for (int m = 0; m < 8; ++m) s[m] = m < nk ? B.cctr[w * K + k0 + m] : absent_sphere();
                 const uint32_t hitk =
                     obstacles_vs_spheres<8, true, false>(sc, bounds_c[part], bounds_c[part + 1], s, nk, flops);
                 // 8 | 32: a chunk's bits never straddle two words
-                if (hitk) {
-                    const int w0 = grouped ? u * kGroupW : u, w1 = grouped ? min(nw, w0 + kGroupW) : u + 1;
-                    for (int w = w0; w < w1; ++w) atomicOr(&B.dirty[w * KW + (k0 >> 5)], hitk << (k0 & 31));
-                }
+                if (hitk) atomicOr(&B.dirty[w * KW + (k0 >> 5)], hitk << (k0 & 31));
             } else {
                 const int r = it - n_cw;
                 const int qq = r / nw, w = r - qq * nw;
@@ -1056,7 +1011,7 @@ __device__ inline uint32_t cc_chunk(const G& g, const Scene& sc, const CcBufs& B
     // then spread them: every dirty pair's obstacle list is cut into n_sub
     // cost-balanced ranges so that the world work makes about two items per
     // thread.
-    const bool compact = gated && !full_sweep && nw * (h.n_sch + h.n_items) <= listcap;
+    const bool compact = gated && !full_sweep && nw * (h.n_sch + h.n_items) <= B.listcap;
     int* wl = reinterpret_cast<int*>(B.pose);  // (sphere chunk << 8 | waypoint) of dirty pairs
     int* sl = wl + nw * h.n_sch;               // (self item << 8 | waypoint) of touching items
     if (compact) {
