@@ -56,6 +56,16 @@ WORKLOAD = ("uneven512: 512 problems, synthetic 7-DOF arm (56 spheres, 960 self 
 METRIC = "plans/s (batched uneven 512-problem workload)"
 
 
+def workload_config(problems) -> dict:
+    """The workload both arms run (their `config`); each arm's own settings go
+    under `arm`."""
+    buckets: dict = {}
+    for p in problems:
+        buckets[str(int(p.max_nodes))] = buckets.get(str(int(p.max_nodes)), 0) + 1
+    return {"workload": WORKLOAD, "problems_per_gpu": len(problems),
+            "buckets": dict(sorted(buckets.items(), key=lambda kv: -int(kv[0])))}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -252,7 +262,10 @@ def run_reference(a):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "plans/s", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * secs / max(1, len(per_step)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_per_step": sample, "parallelism": f"{procs} host processes"},
+        "config": workload_config(problems),
+        "arm": {"sample_per_step": sample, "parallelism": f"{procs} host processes",
+                "planner": "host-driven RRT-Connect (its defaults: binary checker, 16 waypoints per edge, "
+                           "128 samples per iteration, 1000 iterations, 65536 nodes)"},
         "cpu_baseline": {"value": value, "unit": "plans/s", "cores": procs, "kind": "port",
                          "sample": f"<= {sample} problems per step (budget {a.cpu_seconds:.0f} s), host-driven "
                                    f"RRT-Connect restated in C (prrtc_robogpu.py:103-298), {cpu_model()}"},
@@ -430,18 +443,17 @@ def run_ours(a):
         "metric": METRIC, "value": value, "unit": "plans/s", "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": float(np.mean(step_ms)), "higher_is_better": True, "scaling": a.split,
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "problems_per_gpu": len(problems),
-                   "buckets": {str(N): len(ps) for N, ps in buckets.items()},
-                   "tuned": {str(N): v for N, v in tuned.items()},
-                   "collision_checker": settings.collision_checker, "edge_resolution": settings.edge_resolution,
-                   "l2": "flushed (256 MB write) between steps", "gc": "workload frozen (gc.freeze) after set-up",
-                   "launch": ("eager" if a.eager else "CUDA graph replay") + (
-                       ", one launch for all problems with per-problem tree capacities" if a.launch == "merged"
-                       else ", one launch per capacity bucket on concurrent streams"),
-                   "parallelism": (f"weak scaling, {ws} rank(s), every rank its own {len(problems)} problems"
-                                   if a.split == "weak" else
-                                   f"strong scaling, {ws} rank(s), one {a.problems}-problem batch split by "
-                                   "longest-processing-time on estimated cost")},
+        "config": workload_config(problems),
+        "arm": {"tuned": {str(N): v for N, v in tuned.items()},
+                "collision_checker": settings.collision_checker, "edge_resolution": settings.edge_resolution,
+                "l2": "flushed (256 MB write) between steps", "gc": "workload frozen (gc.freeze) after set-up",
+                "launch": ("eager" if a.eager else "CUDA graph replay") + (
+                    ", one launch for all problems with per-problem tree capacities" if a.launch == "merged"
+                    else ", one launch per capacity bucket on concurrent streams"),
+                "parallelism": (f"weak scaling, {ws} rank(s), every rank its own {len(problems)} problems"
+                                if a.split == "weak" else
+                                f"strong scaling, {ws} rank(s), one {a.problems}-problem batch split by "
+                                "longest-processing-time on estimated cost")},
         "success_rate": success,
         "p50_solve_ms": float(np.median(solve_ms)) if solve_ms.size else None,
     }
@@ -465,10 +477,12 @@ def run_ours(a):
         line["e2e"] = {"value": e_solved / e_s, "unit": "plans/s", "h2d_bytes_per_step": int(e_h2d),
                        "d2h_bytes_per_step": int(e_d2h), "steps": e_steps, "rank0_timed_region": e_diag,
                        "api": "prrtc_b200.prrtc_plan_batch_async + .results() (per-problem collision_context "
-                              "dicts, host numpy inputs, one call per step for all of a rank's problems, up to "
-                              "three steps in flight on one stream: later steps are packed and copied while "
-                              "the oldest plans; paths copied to the host; whole job: every rank, slowest "
-                              "rank's time)"}
+                              "dicts, host numpy inputs, one call per step for all of a rank's problems, three "
+                              "steps in flight on one stream: later steps are packed and copied while the "
+                              "oldest plans; paths copied to the host; steady state: the timed window holds "
+                              "exactly `steps` calls (enqueue with its host->device copy) and `steps` "
+                              "read-backs, after 8 untimed steps of the same loop; whole job: every rank, "
+                              "slowest rank's time)"}
 
     if rank == 0 and not a.no_extras:
         # the planners' buffers still hold the last timed step (e2e plans into its own)
@@ -640,8 +654,8 @@ def measure_e2e(torch, dev, planners, settings, tuned, cap_of, steps):
     # One public call per step for all problems, up to three in flight on one
     # stream: the host packs and copies the next steps while the device plans
     # the current one, then reads back the oldest step's results (queued by the
-    # call right behind its own kernels).  Every step's inputs still go host ->
-    # device and its results device -> host inside the timed region.
+    # call right behind its own kernels).  Every timed step's inputs go host ->
+    # device and its results device -> host inside the timed window.
     calls = []
     for key, pl in planners.items():
         ps = pl.problems
@@ -676,49 +690,51 @@ def measure_e2e(torch, dev, planners, settings, tuned, cap_of, steps):
             d2h += pend.d2h_bytes
         return solved, d2h
 
-    def pipeline(n, marks=None):
-        """n steps, depth calls in flight; returns (plans solved, d2h bytes)."""
-        solved = d2h = 0
-        inflight = [enqueue(k) for k in range(min(depth - 1, n))]
-        for k in range(n):
-            if k + depth - 1 < n:
-                inflight.append(enqueue(k + depth - 1))
-            s_, d_ = collect(inflight.pop(0))
-            solved += s_
-            d2h += d_
-            if marks is not None:
-                marks.append(time.perf_counter())
-        return solved, d2h
-
-    # warm with the timed loop itself, so that the caching allocators already
-    # hold every device and pinned block its allocation pattern needs: a
-    # cudaMalloc / cudaHostAlloc inside the timed region costs milliseconds
-    pipeline(2 * depth + 2)
-    torch.cuda.synchronize()
-    _device.H2D_BYTES[0] = 0
     k_e2e = max(1, int(steps))
-    # diagnostics of the timed region: host time per step, device allocations
+    n_warm = 2 * depth + 2
+    # diagnostics of the timed window: host time per step, device allocations
     # (cudaMalloc by the caching allocator) and garbage-collector pauses
     gc_ms = [0.0, 0.0]
 
     def gc_cb(phase, info):
         if phase == "start":
             gc_ms[1] = time.perf_counter()
-        else:
+        elif gc_ms[1] > 0.0:
             gc_ms[0] += (time.perf_counter() - gc_ms[1]) * 1e3
-    gc.callbacks.append(gc_cb)
-    allocs0 = torch.cuda.memory_stats(dev).get("num_device_alloc", 0)
+
+    # One continuous pipeline: depth calls always in flight, the first n_warm
+    # steps untimed (they fill the caching allocators with every device and
+    # pinned block the pattern needs, and the pipeline itself), then a window of
+    # exactly k_e2e enqueues (each with its host -> device copy) and k_e2e
+    # read-backs (each with its device -> host copies), then an untimed drain of
+    # the calls still in flight.
+    solved = d2h = 0
     marks = []
-    t0 = time.perf_counter()
-    solved, d2h = pipeline(k_e2e, marks)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
+    inflight = [enqueue(k) for k in range(depth - 1)]
+    t0 = allocs0 = None
+    for k in range(n_warm + k_e2e):
+        inflight.append(enqueue(k + depth - 1))
+        s_, d_ = collect(inflight.pop(0))
+        if k == n_warm - 1:
+            _device.H2D_BYTES[0] = 0
+            gc.callbacks.append(gc_cb)
+            allocs0 = torch.cuda.memory_stats(dev).get("num_device_alloc", 0)
+            t0 = time.perf_counter()
+        elif k >= n_warm:
+            solved += s_
+            d2h += d_
+            marks.append(time.perf_counter())
+    dt = marks[-1] - t0
+    h2d = _device.H2D_BYTES[0]
     gc.callbacks.remove(gc_cb)
+    allocs = torch.cuda.memory_stats(dev).get("num_device_alloc", 0) - allocs0
+    for pending in inflight:  # drain, untimed
+        collect(pending)
+    torch.cuda.synchronize()
     step_ms = np.diff(np.asarray([t0] + marks)) * 1e3
     diag = {"step_ms_p50": float(np.median(step_ms)), "step_ms_max": float(step_ms.max()),
-            "first_step_ms": float(step_ms[0]), "gc_ms": gc_ms[0],
-            "device_allocs": int(torch.cuda.memory_stats(dev).get("num_device_alloc", 0) - allocs0)}
-    return solved, dt, _device.H2D_BYTES[0] // k_e2e, d2h // k_e2e, k_e2e, diag
+            "gc_ms": gc_ms[0], "device_allocs": int(allocs)}
+    return solved, dt, h2d // k_e2e, d2h // k_e2e, k_e2e, diag
 
 
 def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
