@@ -516,25 +516,43 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     out["fp32_peak_tflops_measured"] = fp32
     out["fp32_probe_tflops"] = rates
 
-    # --- planner roofline: one instrumented (stats) eager step, events around each planner call
+    # --- planner roofline.  Work per launch from the device counters (stats
+    # launches: the counters' atomics slow the kernel, so they are not timed);
+    # the planner kernel's own duration from CUDA events that the library
+    # records right before and after it (tuning.explore_events), over launches
+    # without counters, L2 flushed before each as in the timed region.
     flops = cfgs = edges = nn_nodes = 0
     ms = 0.0
+    n_stat, n_time = 3, 10
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ev1.record()  # creates both events; the library re-records them
+    flush = torch.empty(64 * 2**20, dtype=torch.float32, device=dev)
     for N, pl in planners.items():
         s = PlanSettings(**{**settings.__dict__, **tuned[N]})
         ip = BatchPlanner(pl.problems, cap_of[N], s, dev, stats=True)
         ip.launch()
         torch.cuda.synchronize()
         ip.stats.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        ip.launch()
-        e1.record()
-        e1.synchronize()
-        ms += e0.elapsed_time(e1)
-        st = ip.stats.cpu().numpy()
-        flops += int(st[STAT_FLOPS]); cfgs += int(st[STAT_CONFIGS]); edges += int(st[STAT_EDGES])
-        nn_nodes += int(st[STAT_NN_NODES])
+        for _ in range(n_stat):
+            ip.launch()
+        st = ip.stats.cpu().numpy() / n_stat
+        flops += st[STAT_FLOPS]; cfgs += st[STAT_CONFIGS]; edges += st[STAT_EDGES]
+        nn_nodes += st[STAT_NN_NODES]
         del ip
+        tp = BatchPlanner(pl.problems, cap_of[N], s, dev)
+        tp.tun.explore_events[0], tp.tun.explore_events[1] = ev0.cuda_event, ev1.cuda_event
+        tp.launch()
+        torch.cuda.synchronize()
+        t_ms = []
+        for _ in range(n_time):
+            flush.fill_(1.0)
+            tp.launch()
+            torch.cuda.synchronize()
+            t_ms.append(ev0.elapsed_time(ev1))
+        ms += float(np.mean(t_ms))
+        del tp
+    del flush
     achieved = flops / (ms * 1e-3) / 1e12
     out["roofline"] = {"kernel": "explore_kernel (persistent planner)", "bound": "fp32", "achieved": achieved,
                        "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
@@ -544,7 +562,10 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
                        "traffic": 7.4e6, "traffic_unit": "bytes per launch (ncu)",
                        "peak_source": "measured in bench.py, the faster of the scalar FFMA and packed fma.rn.f32x2 "
                                       "probes (no FP32 entry in MEASURED_PEAKS.json)",
-                       "note": "collision FLOPs actually executed (device counters) / planner time; the planner is "
+                       "launch_ms": ms, "launches_timed": n_time, "launches_counted": n_stat,
+                       "note": "collision FLOPs executed per launch (device counters, mean of 3 launches) / the "
+                               "explore_kernel's own duration (CUDA events recorded around it by the library, mean "
+                               "of 10 launches without counters, L2 flushed before each); the planner is "
                                "latency-bound by its dependent sample->NN->extend->check iterations"}
     out["planner_collision_checks_per_s"] = cfgs / (ms * 1e-3)
     out["planner_edges_per_s"] = edges / (ms * 1e-3)

@@ -181,6 +181,11 @@ typedef struct {
                                     shared-memory carve-out that just holds them, so the rest of
                                     the SM's unified L1 / shared memory serves as L1 for the
                                     trees, radii and scenes; 0 = as many as fit (default) */
+    void* explore_events[2];     /* optional cudaEvent_t pair recorded on the stream right before
+                                    and right after the planner kernel itself (not the fill,
+                                    pack, init and finalize kernels around it), for timing that
+                                    kernel alone; recorded as external event nodes when the
+                                    call is captured into a CUDA graph.  NULL = none */
 } prrtc_tuning_t;
 
 size_t prrtc_b200_plan_workspace_size(const prrtc_inputs_t* in, const prrtc_attrs_t* attrs,

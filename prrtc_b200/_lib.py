@@ -74,7 +74,7 @@ class Tuning(C.Structure):
     _fields_ = [
         ("edge_resolution", F32), ("threads_per_explorer", I32), ("waypoint_chunk", I32),
         ("resident_ctas", I32), ("stats", P), ("point_cloud", P), ("tail_explorers", I32),
-        ("staging_wait_polls", I32), ("ctas_per_sm", I32),
+        ("staging_wait_polls", I32), ("ctas_per_sm", I32), ("explore_events", P * 2),
     ]
 
 

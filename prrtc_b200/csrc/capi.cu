@@ -89,6 +89,7 @@ struct Tuned {
     int tail_join;
     int wait_polls;
     int ctas_per_sm;
+    cudaEvent_t explore_events[2];
 };
 
 static PcView pc_view(const prrtc_point_cloud_t* c) {
@@ -107,7 +108,7 @@ static bool cloud_ok(const prrtc_point_cloud_t* c) {
 }
 
 static Tuned tuned(const prrtc_tuning_t* t) {
-    Tuned o{0.0f, 128, 16, 0, nullptr, nullptr, 1, 0, 0};
+    Tuned o{0.0f, 128, 16, 0, nullptr, nullptr, 1, 0, 0, {nullptr, nullptr}};
     if (t) {
         if (t->edge_resolution > 0.0f) o.edge_res = t->edge_resolution;
         if (t->threads_per_explorer == 32 || t->threads_per_explorer == 64 || t->threads_per_explorer == 128 ||
@@ -121,6 +122,8 @@ static Tuned tuned(const prrtc_tuning_t* t) {
         o.tail_join = t->tail_explorers < 0 ? 0 : 1;
         o.wait_polls = t->staging_wait_polls > 0 ? t->staging_wait_polls : (t->staging_wait_polls < 0 ? -1 : 0);
         o.ctas_per_sm = t->ctas_per_sm > 0 ? t->ctas_per_sm : 0;
+        o.explore_events[0] = static_cast<cudaEvent_t>(t->explore_events[0]);
+        o.explore_events[1] = static_cast<cudaEvent_t>(t->explore_events[1]);
     }
     return o;
 }
@@ -142,6 +145,8 @@ static void fill_launch(PlanLaunch& L, const prrtc_outputs_t* out, const prrtc_a
     L.tail_join = tu.tail_join;
     L.wait_polls = tu.wait_polls;
     L.ctas_per_sm = tu.ctas_per_sm;
+    L.explore_events[0] = tu.explore_events[0];
+    L.explore_events[1] = tu.explore_events[1];
 }
 
 static bool outputs_ok(const prrtc_outputs_t* o) {

@@ -74,6 +74,7 @@ struct PlanLaunch {
     int tail_join;                     // persistent form: idle CTAs join running problems as extra explorers
     int wait_polls;                    // polls of the scene-staging wait before it gives up (0: default, <0: none)
     int ctas_per_sm;                   // persistent form: > 0 caps CTAs per SM and sizes the shared-memory carve-out
+    cudaEvent_t explore_events[2];     // optional, recorded right before / after the planner kernel
     unsigned long long* stats;         // optional device counters (kStat*)
     PcView pc;                         // environment point cloud shared by every problem (pc.n = 0: none)
 };

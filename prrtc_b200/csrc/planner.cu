@@ -779,6 +779,17 @@ size_t device_max_smem() {
     return (size_t)n;
 }
 
+// An optional timing event on the stream; inside a stream capture it becomes an
+// external event-record node, which records each time the graph runs.
+static cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
+    if (!ev) return cudaSuccess;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal)
+                                               : cudaEventRecord(ev, st);
+}
+
 cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
     cudaError_t e;
     {
@@ -835,11 +846,14 @@ cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
         // capacity bucket) a full-GPU grid per launch measured slower, its CTAs
         // piling extra explorers onto a few problems
         grid = std::min<long long>(grid, (long long)L.B * L.E);
+        if ((e = record_event(L.explore_events[0], st)) != cudaSuccess) return e;
         explore_kernel<<<(unsigned)std::max<long long>(grid, 1), L.threads, dyn, st>>>(L);
     } else {
+        if ((e = record_event(L.explore_events[0], st)) != cudaSuccess) return e;
         explore_kernel<<<dim3(L.E, L.B), L.threads, dyn, st>>>(L);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = record_event(L.explore_events[1], st)) != cudaSuccess) return e;
     finalize_kernel<<<(L.B + 127) / 128, 128, 0, st>>>(L);
     return cudaGetLastError();
 }

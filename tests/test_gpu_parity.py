@@ -472,6 +472,32 @@ def test_async_batches_pipelined_on_one_stream(cuda, orc):
                 assert abs(r.cost - np.linalg.norm(np.diff(path, axis=0), axis=1).sum()) < 1e-3 * max(1.0, r.cost)
 
 
+def test_explore_events_time_the_planner_kernel(cuda):
+    """tuning.explore_events: the library records the pair right around the
+    planner kernel, eagerly and as external event nodes of a captured graph, so
+    the span is positive and shorter than the whole planner call."""
+    from prrtc_b200.batch import BatchPlanner, PlanSettings
+
+    probs = [make_problem("uneven", 600 + i) for i in range(6)]
+    pl = BatchPlanner(probs, [p.max_nodes for p in probs], PlanSettings(num_new_samples=2), cuda)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ev1.record()
+    pl.tun.explore_events[0], pl.tun.explore_events[1] = ev0.cuda_event, ev1.cuda_event
+    for graph in (False, True):
+        if graph:
+            pl.capture()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record()
+        pl.run()
+        c1.record()
+        c1.synchronize()
+        k_ms, call_ms = ev0.elapsed_time(ev1), c0.elapsed_time(c1)
+        assert 0.0 < k_ms <= call_ms, (graph, k_ms, call_ms)
+        assert (pl.summary_block()[:, 8] == 1).sum().item() >= len(probs) - 1
+    pl.graph = None
+
+
 def test_result_block_and_packed_paths(cuda):
     """prrtc_b200_result_block through the C-ABI against a numpy restatement:
     1500 problems (two chunks of the one-CTA scan), unsolved, failed, empty and
