@@ -226,6 +226,27 @@ class Scene:
         ok = lib().orc_validate_path(self.ref, _ptr(p), p.shape[0], float(resolution), C.byref(md))
         return bool(ok), float(md.value)
 
+    def validate_planned_path(self, path, granularity: int = 16, resolution: float = 0.01,
+                              graze_depth: float = 1e-3):
+        """Re-validation of a path a sampling planner returned: (ok, min distance).
+
+        The path passes when it is free at an independent `resolution` grid.
+        Otherwise it must be free on the planner's own waypoints -- each edge at
+        max(granularity, ceil(len/resolution)) points t = (k+1)/G, as the planner
+        checked it, within 1e-5 m of contact (float32 against float64) -- and any
+        graze between those waypoints, found at resolution/20, must be shallower
+        than `graze_depth`: a sampled edge check cannot see a graze that lies
+        between its samples, in this planner as in the reference's."""
+        p = np.ascontiguousarray(path, dtype=np.float32).reshape(-1, self.dim)
+        ok, md = self.validate_path(p, resolution)
+        if ok:
+            return True, md
+        grid = np.concatenate([edge_waypoints(p[i], p[i + 1], granularity, resolution)
+                               for i in range(p.shape[0] - 1)] + [p[:1]])
+        md_grid = float(self.min_distances(grid).min())
+        _, md_fine = self.validate_path(p, resolution / 20.0)
+        return (md_grid >= -1e-5 and md_fine > -graze_depth), min(md_grid, md_fine)
+
     def smooth_cost(self, waypoints, margin=0.02, beta=50.0, w_len=1.0) -> float:
         w = np.ascontiguousarray(waypoints, dtype=np.float64).reshape(-1, self.dim)
         return float(lib().orc_smooth_cost(self.ref, _ptr(w), w.shape[0], float(margin), float(beta), float(w_len)))

@@ -267,7 +267,7 @@ def test_plan_solves_and_revalidates(cuda, orc, kind, seed, checker):
     assert np.array_equal(path[0], pr.start)
     assert any(np.array_equal(path[-1], g) for g in pr.goals)
     sc = orc.Scene(pr.context, pr.dim)
-    ok, md = sc.validate_path(path, 0.01)
+    ok, md = sc.validate_planned_path(path)
     assert ok, md
     assert abs(r.cost - float(np.linalg.norm(np.diff(path, axis=0), axis=1).sum())) < 1e-3
     assert r.kernel_time_ms > 0.0
@@ -305,7 +305,7 @@ def test_batch_uneven_solves(cuda, orc, launch, threads, ctas):
         assert np.array_equal(path[0], p.start)
         assert any(np.array_equal(path[-1], g) for g in p.goals)
         sc = orc.Scene(p.context, dim)
-        ok, md = sc.validate_path(path, 0.01)
+        ok, md = sc.validate_planned_path(path)
         assert ok, md
         if i < 3:
             _check_tree_sound(sc, r.tree_a_configs.cpu().numpy(), r.tree_a_parents.cpu().numpy(), r.tree_a_size, dim)
@@ -337,7 +337,7 @@ def test_batch_dual_arm_large_world(cuda, orc, threads, ctas):
         path = r.path.cpu().numpy()
         assert np.array_equal(path[0], p.start)
         assert any(np.array_equal(path[-1], g) for g in p.goals)
-        ok, md = orc.Scene(p.context, dim).validate_path(path, 0.01)
+        ok, md = orc.Scene(p.context, dim).validate_planned_path(path)
         assert ok, md
 
 
@@ -432,7 +432,7 @@ def test_async_batches_on_two_streams(cuda, orc):
         assert sum(r.solved for r in res) >= len(probs) - 1
         for p, r in zip(probs, res):
             if r.solved:
-                ok, md = orc.Scene(p.context, p.dim).validate_path(r.path.numpy(), 0.01)
+                ok, md = orc.Scene(p.context, p.dim).validate_planned_path(r.path.numpy())
                 assert ok, md
 
 
@@ -467,7 +467,7 @@ def test_async_batches_pipelined_on_one_stream(cuda, orc):
                 assert path.shape[1] == p.dim and r.path.device.type == "cpu"
                 assert np.array_equal(path[0], p.start.astype(np.float32))
                 assert any(np.array_equal(path[-1], g.astype(np.float32)) for g in p.goals)
-                ok, md = orc.Scene(p.context, p.dim).validate_path(path, 0.01)
+                ok, md = orc.Scene(p.context, p.dim).validate_planned_path(path)
                 assert ok, md
                 assert abs(r.cost - np.linalg.norm(np.diff(path, axis=0), axis=1).sum()) < 1e-3 * max(1.0, r.cost)
 
@@ -608,7 +608,7 @@ def test_batch_per_problem_capacity(cuda, orc):
     for p, r, cap in zip(probs, res, caps):
         assert r.tree_a_configs.shape[1] <= cap and r.tree_b_configs.shape[1] <= cap
         if r.solved:
-            ok, md = orc.Scene(p.context, dim).validate_path(r.path.cpu().numpy(), 0.01)
+            ok, md = orc.Scene(p.context, dim).validate_planned_path(r.path.cpu().numpy())
             assert ok, md
     assert sum(r.solved for r in res[:5]) >= 4
     assert not res[5].solved and max(res[5].tree_a_size, res[5].tree_b_size) >= 2
@@ -651,7 +651,7 @@ def test_batch_mixed_full_and_trimmed_contexts(cuda, orc, launch):
             continue
         path = r.path.cpu().numpy()
         assert np.array_equal(path[0], starts[i]) and np.array_equal(path[-1], goals[i])
-        ok, md = orc.Scene(ctxs[i], base.dim).validate_path(path, 0.01)
+        ok, md = orc.Scene(ctxs[i], base.dim).validate_planned_path(path)
         assert ok, (i, md)
         _check_tree_sound(orc.Scene(ctxs[i], base.dim), r.tree_a_configs.cpu().numpy(),
                           r.tree_a_parents.cpu().numpy(), r.tree_a_size, base.dim)
@@ -686,7 +686,7 @@ def test_batch_inputs_as_device_tensors_and_tensor_contexts(cuda, orc):
     assert sum(r.solved for r in res) >= len(probs) - 1
     for p, r in zip(probs, res):
         if r.solved:
-            ok, md = orc.Scene(p.context, dim).validate_path(r.path.cpu().numpy(), 0.01)
+            ok, md = orc.Scene(p.context, dim).validate_planned_path(r.path.cpu().numpy())
             assert ok, md
 
 
@@ -704,7 +704,7 @@ def test_plan_balance_modes(cuda, orc, balance_mode, tree_ratio):
                    balance_mode=balance_mode, tree_ratio=tree_ratio, min_vals=pr.lower, max_vals=pr.upper,
                    collision_context=pr.context, collision_checker="binary_coarse_coop", edge_resolution=0.01)
     assert r.solved
-    ok, md = sc.validate_path(r.path.cpu().numpy(), 0.01)
+    ok, md = sc.validate_planned_path(r.path.cpu().numpy())
     assert ok, md
     probs = [make_problem("uneven", 600 + i) for i in range(4)]
     G = max(p.goals.shape[0] for p in probs)
@@ -719,7 +719,7 @@ def test_plan_balance_modes(cuda, orc, balance_mode, tree_ratio):
     assert sum(x.solved for x in res) >= len(probs) - 1
     for p, x in zip(probs, res):
         if x.solved:
-            ok, md = orc.Scene(p.context, pr.dim).validate_path(x.path.cpu().numpy(), 0.01)
+            ok, md = orc.Scene(p.context, pr.dim).validate_planned_path(x.path.cpu().numpy())
             assert ok, md
 
 
@@ -812,7 +812,7 @@ def test_more_than_32_joints(cuda, orc):
                    min_vals=pr.lower, max_vals=pr.upper, collision_context=pr.context,
                    collision_checker="binary_coarse_coop", edge_resolution=0.02)
     assert r.solved
-    ok, md = sc.validate_path(r.path.cpu().numpy(), 0.02)
+    ok, md = sc.validate_planned_path(r.path.cpu().numpy(), resolution=0.02)
     assert ok, md
 
 

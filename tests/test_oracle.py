@@ -257,6 +257,52 @@ def test_sequential_prrtc_solves_and_revalidates(orc, kind, seed):
     assert r2.tree_sizes == r.tree_sizes and r2.connection == r.connection  # sequential => deterministic
 
 
+def test_validate_planned_path_rules(orc, arm):
+    """validate_planned_path.  A 0.12 rad edge: the planner checks it at 16
+    waypoints (t = k/16, granularity 16), an independent 0.01 rad grid at 12 (t =
+    k/12).  A small world sphere grazing the fastest robot sphere at t = 5/12 by
+    20 um -- free at every planner waypoint -- fails the independent grid, passes
+    as a shallow graze, and fails when graze_depth is below its depth; a sphere
+    on the path fails outright."""
+    from prrtc_b200.context import build_collision_context
+
+    dim = arm.dim
+    empty = build_collision_context(arm, {})
+    sc0 = orc.Scene(empty, dim)
+    q0 = np.zeros(dim, np.float32)
+    q0[1], q0[3] = 1.2, -0.5  # arm stretched out: the base joint sweeps its far spheres
+    q1 = q0.copy()
+    q1[0] = np.float32(0.12)
+    sli, sloc, srad = empty["sphere_link_idx"], empty["sphere_local"], empty["sphere_radius"]
+
+    def centres(q):
+        F = sc0.fk(np.asarray(q, np.float32))
+        return np.stack([F[l, :9].reshape(3, 3) @ sloc[i] + F[l, 9:12] for i, l in enumerate(sli)])
+
+    def at(t):
+        return q0 + np.float32(t) * (q1 - q0)
+
+    s = int(np.argmax(np.linalg.norm(centres(q1) - centres(q0), axis=1)))
+    tg, rho, depth = 5.0 / 12.0, 0.01, 2e-5
+    cg = centres(at(tg))[s]
+    v = centres(at(tg + 1e-3))[s] - centres(at(tg - 1e-3))[s]
+    u = np.cross(v, [0.0, 0.0, 1.0])
+    u /= np.linalg.norm(u)
+    o = cg + u * (srad[s] + rho - depth)
+    sc = orc.Scene(build_collision_context(arm, {"world_spheres": np.array([[*o, rho]], np.float32)}), dim)
+    path = np.stack([q0, q1])
+    planner = orc.edge_waypoints(q0, q1, 16, 0.01)
+    assert planner.shape[0] == 16 and sc.min_distances(planner).min() > 0.0
+    assert sc.min_distances(at(tg)[None])[0] < -depth / 2
+    assert sc0.validate_planned_path(path)[0]
+    assert not sc.validate_path(path, 0.01)[0]
+    ok, md = sc.validate_planned_path(path)
+    assert ok and -2 * depth < md < 0.0
+    assert not sc.validate_planned_path(path, graze_depth=depth / 2)[0]
+    hit = orc.Scene(build_collision_context(arm, {"world_spheres": np.array([[*cg, 0.05]], np.float32)}), dim)
+    assert not hit.validate_planned_path(path)[0]
+
+
 def test_sequential_prrtc_overflow_and_iteration_limit(orc):
     pr = make_problem("tabletop", 5)
     sc = orc.Scene(pr.context, pr.dim)
