@@ -487,8 +487,14 @@ def run_ours(a):
     if rank == 0 and not a.no_extras:
         # the planners' buffers still hold the last timed step (e2e plans into its own)
         line.update(revalidate_step(planners))
-        line.update(extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of))
-        line.update(measure_configs(a, torch, lib, dev, settings, tuned))
+        if ws == 1:
+            # single-GPU side measurements (kernels, CPU baseline, the other
+            # workloads) only at N = 1: at N > 1 the other ranks would wait for
+            # them at the closing barrier
+            line.update(extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of))
+            line.update(measure_configs(a, torch, lib, dev, settings, tuned))
+        else:
+            line.update(planner_roofline(torch, lib, dev, planners, settings, tuned, cap_of))
     if rank == 0:
         line["clocks"] = clk.summary()
         print(json.dumps(line))
@@ -500,17 +506,12 @@ def run_ours(a):
     return 0
 
 
-def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of):
-    """Side measurements on rank 0: roofline of the planner kernel, e2e through the
-    public API, the plain per-problem launch form, standalone CC and NN kernels,
-    and the CPU baseline."""
-    from prrtc_b200 import _lib as L
+def planner_roofline(torch, lib, dev, planners, settings, tuned, cap_of):
+    """Roofline of the dominant kernel (explore_kernel) against the FP32 peak
+    measured by the FFMA probes, with the planner's device counters."""
     from prrtc_b200.batch import STAT_CONFIGS, STAT_EDGES, STAT_FLOPS, STAT_NN_NODES, BatchPlanner, PlanSettings
-    from prrtc_b200.collision import CollisionChecker
-    from prrtc_b200.prrtc import prrtc_nearest_neighbor, prrtc_plan_batch, prrtc_plan_batch_async
 
     out = {}
-    peaks = measured_peaks()
     rates = fp32_probe_rates(torch, lib, dev)
     fp32 = max(rates.values())
     out["fp32_peak_tflops_measured"] = fp32
@@ -570,6 +571,19 @@ def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of
     out["planner_collision_checks_per_s"] = cfgs / (ms * 1e-3)
     out["planner_edges_per_s"] = edges / (ms * 1e-3)
     out["planner_nn_gbs"] = nn_nodes * 7 * 4 / (ms * 1e-3) / 1e9
+
+    return out
+
+
+def extras(a, torch, lib, dev, problems, planners, settings, tuned, line, cap_of):
+    """Side measurements on rank 0 at N = 1: roofline of the planner kernel, the
+    plain per-problem launch form, standalone CC and NN kernels, and the CPU
+    baseline."""
+    from prrtc_b200.prrtc import prrtc_plan_batch
+
+    out = planner_roofline(torch, lib, dev, planners, settings, tuned, cap_of)
+    peaks = measured_peaks()
+    fp32 = out["fp32_peak_tflops_measured"]
 
     # --- plain per-problem-launch form (the reference's batch structure) on the same GPU
     from prrtc_b200.batch import bucket_problems
