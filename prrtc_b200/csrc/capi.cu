@@ -155,6 +155,31 @@ static bool outputs_ok(const prrtc_outputs_t* o) {
            o->kernel_time_ms;
 }
 
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// A driver entry point looked up through the runtime (no link against libcuda).
+static void* driver_entry(const char* name) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+        p = nullptr;
+    return p;
+}
+
+// The current CUDA context's identity: cuCtxGetId, unique to each creation of a
+// context (the primary context re-created after cudaDeviceReset gets a new id,
+// while its handle may be the old one), else the handle itself; 0 = unknown.
+unsigned long long prrtc::current_context_key() {
+    static const auto get_ctx = reinterpret_cast<CtxGetCurrentFn>(driver_entry("cuCtxGetCurrent"));
+    static const auto get_id = reinterpret_cast<CtxGetIdFn>(driver_entry("cuCtxGetId"));
+    CUcontext ctx = nullptr;
+    if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS || !ctx) return 0ull;
+    unsigned long long id = 0ull;
+    if (get_id && get_id(ctx, &id) == CUDA_SUCCESS && id != 0ull) return id;
+    return static_cast<unsigned long long>(reinterpret_cast<uintptr_t>(ctx));
+}
+
 extern "C" {
 
 int prrtc_b200_version(void) { return 1; }
@@ -567,23 +592,7 @@ static std::mutex g_noalloc_mutex;
 // Device address of g_noalloc_scene per device ordinal, with the CUDA context it
 // belongs to: the address is valid only in that context.
 static unsigned char* g_noalloc_ptr[256];
-static CUcontext g_noalloc_ctx[256];
-
-typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
-
-// The driver's cuCtxGetCurrent, looked up through the runtime (no link against
-// libcuda): the context a device address belongs to.
-static CtxGetCurrentFn ctx_get_current() {
-    static CtxGetCurrentFn fn = [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            p = nullptr;
-        return reinterpret_cast<CtxGetCurrentFn>(p);
-    }();
-    return fn;
-}
+static unsigned long long g_noalloc_ctx[256];  // context key of each cached address
 
 // Host code cannot use g_noalloc_scene's name as a device address: resolve it
 // with the device current, once per device and context.  A call made in a
@@ -595,17 +604,15 @@ static int noalloc_scene_ptr(unsigned char** out) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e);
     if (dev < 0 || dev >= 256) return PRRTC_B200_EUNSUPPORTED;
-    const CtxGetCurrentFn get_ctx = ctx_get_current();
-    CUcontext ctx = nullptr;
-    if (get_ctx && get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
+    unsigned long long key = current_context_key();
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
+    if (!g_noalloc_ptr[dev] || !key || key != g_noalloc_ctx[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scene);  // makes the device's primary context current if none is
         if (e != cudaSuccess) return cuda_fail(e);
-        if (get_ctx && get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
+        key = current_context_key();
         g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
-        g_noalloc_ctx[dev] = ctx;
+        g_noalloc_ctx[dev] = key;
     }
     *out = g_noalloc_ptr[dev];
     return PRRTC_B200_OK;

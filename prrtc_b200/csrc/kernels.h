@@ -79,6 +79,10 @@ struct PlanLaunch {
     PcView pc;                         // environment point cloud shared by every problem (pc.n = 0: none)
 };
 
+// Identity of the calling thread's current CUDA context (cuCtxGetId, else the
+// handle), 0 when unknown (capi.cu).
+unsigned long long current_context_key();
+
 size_t plan_workspace_bytes(int B, int N, size_t blob_stride);
 void plan_carve_workspace(PlanLaunch& L, void* ws, size_t blob_stride);
 cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st);

@@ -28,6 +28,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "kernels.h"
 #include "prrtc_device.cuh"
@@ -779,6 +780,19 @@ size_t device_max_smem() {
     return (size_t)n;
 }
 
+// explore_kernel's attributes as last set in one device's CUDA context.
+struct ExploreAttrs {
+    unsigned long long ctx = 0ull;  // context key (current_context_key)
+    int max_dyn = -1;          // largest MaxDynamicSharedMemorySize set
+    int carve = INT_MIN;       // carve-out preference set (-1 = none)
+    bool have_smem = false;    // the three sizes below are known
+    int sm_smem = 0, reserved = 0;
+    size_t static_smem = 0;
+};
+constexpr int kMaxCachedDevices = 256;
+static ExploreAttrs g_explore_attr[kMaxCachedDevices];
+static std::mutex g_explore_attr_mutex;
+
 // An optional timing event on the stream; inside a stream capture it becomes an
 // external event-record node, which records each time the graph runs.
 static cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
@@ -810,29 +824,55 @@ cudaError_t launch_plan(PlanLaunch& L, cudaStream_t st) {
         L.blob_cap = 0;
         dyn = cc;
     }
-    if ((e = cudaFuncSetAttribute(explore_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) !=
-        cudaSuccess)
-        return e;
     // ctas_per_sm > 0: the smallest shared-memory carve-out that holds that many
     // CTAs, so the rest of the SM's unified L1 / shared memory is L1 (the
     // explorers read trees, radii and unstaged scene data through it); measured
-    // faster than the largest carve-out's one more resident CTA per SM.  The
-    // attribute belongs to the kernel, so every launch sets it (-1: no preference).
-    int carve = -1;
-    if (L.persistent && L.ctas_per_sm > 0) {
-        int dev = 0, sm_smem = 0, reserved = 0;
-        cudaFuncAttributes fa;
-        cudaGetDevice(&dev);
-        if ((e = cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess ||
-            (e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess ||
-            (e = cudaFuncGetAttributes(&fa, explore_kernel)) != cudaSuccess)
-            return e;
-        const size_t need = (size_t)L.ctas_per_sm * (dyn + fa.sharedSizeBytes + (size_t)reserved);
-        carve = sm_smem > 0 ? (int)std::min<size_t>(100, (100 * need + sm_smem - 1) / (size_t)sm_smem) : -1;
+    // faster than the largest carve-out's one more resident CTA per SM (-1: no
+    // preference).  The kernel's attributes are set only when they change, from
+    // a cache per device and CUDA context: querying or setting them while the
+    // previous batch's planner still ran measured as a host-side wait for that
+    // launch, which serialised back-to-back calls (e2e 134 K against 198 K
+    // plans/s with a carve-out set on every call).
+    {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        const unsigned long long ctx = current_context_key();
+        std::lock_guard<std::mutex> lock(g_explore_attr_mutex);
+        ExploreAttrs dflt;
+        ExploreAttrs& c = (dev >= 0 && dev < kMaxCachedDevices) ? g_explore_attr[dev] : dflt;
+        if (!ctx || c.ctx != ctx) {
+            c = ExploreAttrs{};
+            c.ctx = ctx;
+        }
+        if ((int)dyn > c.max_dyn) {
+            if ((e = cudaFuncSetAttribute(explore_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) !=
+                cudaSuccess)
+                return e;
+            c.max_dyn = (int)dyn;
+        }
+        int carve = -1;
+        if (L.persistent && L.ctas_per_sm > 0) {
+            if (!c.have_smem) {
+                cudaFuncAttributes fa;
+                if ((e = cudaDeviceGetAttribute(&c.sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) !=
+                        cudaSuccess ||
+                    (e = cudaDeviceGetAttribute(&c.reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) !=
+                        cudaSuccess ||
+                    (e = cudaFuncGetAttributes(&fa, explore_kernel)) != cudaSuccess)
+                    return e;
+                c.static_smem = fa.sharedSizeBytes;
+                c.have_smem = true;
+            }
+            const size_t need = (size_t)L.ctas_per_sm * (dyn + c.static_smem + (size_t)c.reserved);
+            carve = c.sm_smem > 0 ? (int)std::min<size_t>(100, (100 * need + c.sm_smem - 1) / (size_t)c.sm_smem) : -1;
+        }
+        if (carve != c.carve) {
+            if ((e = cudaFuncSetAttribute(explore_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carve)) !=
+                cudaSuccess)
+                return e;
+            c.carve = carve;
+        }
     }
-    if ((e = cudaFuncSetAttribute(explore_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, carve)) !=
-        cudaSuccess)
-        return e;
     if (L.persistent) {
         int per_sm = 0;
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, explore_kernel, L.threads, dyn)) !=
