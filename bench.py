@@ -779,22 +779,31 @@ def measure_e2e(torch, dev, planners, settings, tuned, cap_of, steps):
     return solved, dt, h2d // k_e2e, d2h // k_e2e, k_e2e, diag
 
 
-def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
-    """Standalone FK + collision kernel, flat checker, full sweep: FP32 roofline."""
-    from prrtc_b200 import scenes
-    from prrtc_b200.collision import CollisionChecker
-    from prrtc_b200.context import build_collision_context
+def _cc_flops(ctx) -> tuple[int, int]:
+    """Algorithmic FP32 flops (FFMA = 2) and pair tests of one full-sweep check
+    of a configuration against the scene of `ctx`, per the kernel's own
+    per-test constants (prrtc_device.cuh kFlop*): FK J*(90+63) + S*18 sphere
+    centres + S*(Ns*8 + Nc*23 + Nb*26 + Nh*6) world tests + P*8 self pairs."""
+    J = int(np.asarray(ctx["fk_twists"]).reshape(-1, 6).shape[0])
+    S = int(np.asarray(ctx["sphere_radius"]).reshape(-1).shape[0])
+    P = int(np.asarray(ctx["self_pairs"]).reshape(-1, 2).shape[0])
+    ns, nc, nb, nh = (int(np.asarray(ctx[k]).shape[0]) if np.asarray(ctx[k]).size else 0
+                      for k in ("world_spheres", "world_capsules", "world_boxes", "world_halfspaces"))
+    flops = J * (90 + 63) + S * 18 + S * (ns * 8 + nc * 23 + nb * 26 + nh * 6) + P * 8
+    return flops, S * (ns + nc + nb + nh) + P
 
-    rng = np.random.default_rng(0)
-    ctx = build_collision_context(scenes.arm(0), scenes.tabletop_world(rng))
-    chk = CollisionChecker(ctx, 7, "binary", 0.0, dev)
-    n = configs
-    q = torch.from_numpy(rng.uniform(-2.8, 2.8, (n, 7)).astype(np.float32)).to(dev)
+
+def _time_cc(torch, dev, ctx, dim, lo, hi, n, reps, rng, profile=False):
+    from prrtc_b200.collision import CollisionChecker
+
+    chk = CollisionChecker(ctx, dim, "binary", 0.0, dev)
+    q = torch.from_numpy(rng.uniform(lo, hi, (n, dim)).astype(np.float32)).to(dev)
     outv = torch.empty(n, dtype=torch.int32, device=dev)
     chk.check(q, full_sweep=True, out=outv)
     torch.cuda.synchronize()
     best = 1e30
-    torch.cuda.profiler.start()
+    if profile:
+        torch.cuda.profiler.start()
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -802,19 +811,51 @@ def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
         e1.record()
         e1.synchronize()
         best = min(best, e0.elapsed_time(e1))
-    torch.cuda.profiler.stop()
-    # per-test FP32 flops as issued by the kernel (prrtc_device.cuh kFlop* constants)
-    S, P = 56, 960
-    ns, nc, nb, nh = 32, 8, 20, 1
-    f_cfg = 7 * (90 + 63) + S * 18 + S * (ns * 8 + nc * 23 + nb * 26 + nh * 6) + P * 8
+    if profile:
+        torch.cuda.profiler.stop()
+    return best, float(outv.float().mean().item())
+
+
+def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
+    """Standalone FK + collision kernel, flat checker, full sweep: FP32 roofline
+    on the tabletop scene (config 2), and on the scenes of config 1 (16 world
+    spheres) and config 5 (dual arm, 256 spheres + 64 boxes + floor)."""
+    from prrtc_b200 import scenes
+    from prrtc_b200.context import build_collision_context
+
+    rng = np.random.default_rng(0)
+    arm = scenes.arm(0)
+    ctx = build_collision_context(arm, scenes.tabletop_world(rng))
+    n = configs
+    # the profiled launches (ncu --profile-from-start off) are the tabletop ones
+    best, _ = _time_cc(torch, dev, ctx, 7, -2.8, 2.8, n, reps, rng, profile=True)
+    f_cfg, _ = _cc_flops(ctx)
     ach = n * f_cfg / (best * 1e-3) / 1e12
-    return {"cc_kernel": {"workload": f"tabletop scene (32 spheres, 8 capsules, 20 boxes, 1 halfspace), {n} configs, "
-                                      "flat checker, full sweep", "checks_per_s": n / (best * 1e-3),
-                          "flops_per_check": f_cfg, "achieved_tflops": ach,
-                          "frac_of_fp32_peak": (ach / fp32) if fp32 else None,
-                          # one ncu capture (profiles/check_kernel_tabletop_fullsweep.md): the
-                          # configurations, read once; the scene lives in shared memory
-                          "traffic_bytes_ncu": 29.45e6}}
+    out = {"cc_kernel": {"workload": f"tabletop scene (32 spheres, 8 capsules, 20 boxes, 1 halfspace), {n} configs, "
+                                     "flat checker, full sweep", "checks_per_s": n / (best * 1e-3),
+                         "flops_per_check": f_cfg, "achieved_tflops": ach,
+                         "frac_of_fp32_peak": (ach / fp32) if fp32 else None,
+                         # one ncu capture (profiles/check_kernel_tabletop_fullsweep.md): the
+                         # configurations, read once; the scene lives in shared memory
+                         "traffic_bytes_ncu": 29.45e6}}
+    dual = scenes.dual_arm(0)
+    others = {}
+    for key, robot, world, what in (
+            ("config1_spheres16", arm, scenes.spheres_world(np.random.default_rng(1), 16),
+             "7-DOF arm (56 spheres, 960 self pairs), 16 world spheres"),
+            ("config5_dual_arm", dual, scenes.large_world(np.random.default_rng(2)),
+             "dual arm (14 DOF + 4 mimic joints, 120 spheres), 256 spheres + 64 boxes + floor")):
+        c = build_collision_context(robot, world)
+        dim = int(robot.lower.shape[0])
+        t, coll = _time_cc(torch, dev, c, dim, robot.lower, robot.upper, n, reps, rng)
+        f, pairs = _cc_flops(c)
+        a_ = n * f / (t * 1e-3) / 1e12
+        others[key] = {"workload": f"{what}, {n} uniform configurations, flat checker, full sweep",
+                       "checks_per_s": n / (t * 1e-3), "flops_per_check": f, "pair_tests_per_check": pairs,
+                       "achieved_tflops": a_, "frac_of_fp32_peak": (a_ / fp32) if fp32 else None,
+                       "in_collision": coll}
+    out["cc_kernel_other_scenes"] = others
+    return out
 
 
 def measure_smooth(torch, dev, paths: int = 512, waypoints: int = 64, launches: int = 20, reps: int = 3):

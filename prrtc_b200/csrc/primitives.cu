@@ -337,12 +337,15 @@ __global__ void __launch_bounds__(128, PRRTC_CHECK_MINBLOCKS) check_kernel(const
     }
 }
 
-cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t* pairs, int J, int S, int K,
-                         int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
-                         cudaStream_t st, const PcView* pc) {
-    if (n <= 0) return cudaSuccess;
-    const PcView cloud = pc ? *pc : PcView{nullptr, nullptr, 0, 0, 0.0f, 0.0f};
-    constexpr int CW = PRRTC_CHECK_CW;
+// One candidate pass size of the batched checker: its kernel, dynamic shared
+// memory (the scene staged when it fits), and resident CTAs per SM.
+struct CheckLaunch {
+    int cw = 0, blob_cap = 0, per_sm = 0;
+    size_t dyn = 0;
+};
+
+template <int CW>
+static cudaError_t check_option(int full_sweep, int J, int S, int K, int Q, int blob_cap, CheckLaunch& o) {
     const size_t cc = (size_t)cc_smem_bytes(J, S, K, Q, CW);
     size_t dyn = cc + (size_t)blob_cap;
     if (dyn + 64 > device_max_smem()) {
@@ -354,9 +357,63 @@ cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t*
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, dyn)) != cudaSuccess) return e;
+    o.cw = CW;
+    o.blob_cap = blob_cap;
+    o.per_sm = per_sm;
+    o.dyn = dyn;
+    return cudaSuccess;
+}
+
+template <int CW>
+static void check_go(const CheckLaunch& o, int full_sweep, const unsigned char* blob, const int32_t* pairs, int J,
+                     int S, int K, int Q, int dim, const float* configs, int n, int32_t* verdicts, cudaStream_t st,
+                     const PcView& cloud) {
     const long long chunks = (n + CW - 1) / CW;
-    const long long grid = std::min<long long>(chunks, (long long)std::max(per_sm, 1) * device_sm_count());
-    kern<<<(unsigned)grid, 128, dyn, st>>>(blob, blob_cap, pairs, J, S, K, Q, dim, configs, n, verdicts, cloud);
+    const long long grid = std::min<long long>(chunks, (long long)std::max(o.per_sm, 1) * device_sm_count());
+    auto kern = full_sweep ? check_kernel<CW, true> : check_kernel<CW, false>;
+    kern<<<(unsigned)grid, 128, o.dyn, st>>>(blob, o.blob_cap, pairs, J, S, K, Q, dim, configs, n, verdicts, cloud);
+}
+
+// Passes of PRRTC_CHECK_CW configurations, unless their buffers leave fewer
+// than PRRTC_CHECK_MINBLOCKS CTAs per SM (large robots: the sphere centres and
+// link frames of a pass grow with S and J); then half or a quarter as many
+// configurations per pass, whichever keeps the most CTAs resident (the larger
+// pass on a tie).  The dual arm with 120 spheres fits one CTA per SM at 32
+// configurations per pass and three at 16: 43.9 -> 60.2 M checks/s.
+cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t* pairs, int J, int S, int K,
+                         int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
+                         cudaStream_t st, const PcView* pc) {
+    if (n <= 0) return cudaSuccess;
+    const PcView cloud = pc ? *pc : PcView{nullptr, nullptr, 0, 0, 0.0f, 0.0f};
+    constexpr int CW = PRRTC_CHECK_CW;
+    CheckLaunch best, o;
+    cudaError_t e = check_option<CW>(full_sweep, J, S, K, Q, blob_cap, best);
+    if (e != cudaSuccess) return e;
+    if constexpr (CW / 2 >= 8) {
+        if (best.per_sm < PRRTC_CHECK_MINBLOCKS) {
+            if ((e = check_option<CW / 2>(full_sweep, J, S, K, Q, blob_cap, o)) != cudaSuccess) return e;
+            if (o.per_sm > best.per_sm) best = o;
+        }
+    }
+    if constexpr (CW / 4 >= 8) {
+        if (best.per_sm < PRRTC_CHECK_MINBLOCKS) {
+            if ((e = check_option<CW / 4>(full_sweep, J, S, K, Q, blob_cap, o)) != cudaSuccess) return e;
+            if (o.per_sm > best.per_sm) best = o;
+        }
+    }
+    if constexpr (CW / 2 >= 8) {
+        if (best.cw == CW / 2) {
+            check_go<CW / 2>(best, full_sweep, blob, pairs, J, S, K, Q, dim, configs, n, verdicts, st, cloud);
+            return cudaGetLastError();
+        }
+    }
+    if constexpr (CW / 4 >= 8) {
+        if (best.cw == CW / 4) {
+            check_go<CW / 4>(best, full_sweep, blob, pairs, J, S, K, Q, dim, configs, n, verdicts, st, cloud);
+            return cudaGetLastError();
+        }
+    }
+    check_go<CW>(best, full_sweep, blob, pairs, J, S, K, Q, dim, configs, n, verdicts, st, cloud);
     return cudaGetLastError();
 }
 
