@@ -1414,7 +1414,8 @@ def measure_plain_device(torch, dev, problems, settings, n_streams=8):
 
 
 def measure_configs(a, torch, lib, dev, settings, tuned):
-    """The other BASELINE configurations, rank 0, after the headline."""
+    """The other workloads (single plan, 1000 tabletop plans, smoothing, dual arm, dense batch), rank 0,
+    after the headline."""
     from prrtc_b200.batch import PlanSettings
 
     want = set(x.strip() for x in a.configs.split(",")) - {"none", ""}
