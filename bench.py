@@ -818,8 +818,8 @@ def _time_cc(torch, dev, ctx, dim, lo, hi, n, reps, rng, profile=False):
 
 def measure_cc(torch, dev, fp32, configs: int = 1 << 20, reps: int = 3):
     """Standalone FK + collision kernel, flat checker, full sweep: FP32 roofline
-    on the tabletop scene (config 2), and on the scenes of config 1 (16 world
-    spheres) and config 5 (dual arm, 256 spheres + 64 boxes + floor)."""
+    on the tabletop scene, on the single-plan scene (arm, 16 world spheres) and
+    on the dual-arm scene (120 spheres, 256 spheres + 64 boxes + floor)."""
     from prrtc_b200 import scenes
     from prrtc_b200.context import build_collision_context
 
