@@ -329,15 +329,6 @@ class _Results:
         return torch.stack(nodes, 0).to(self.paths.device)
 
 
-def _limits(min_vals, max_vals, dim, device):
-    if min_vals is None:
-        min_vals = torch.full((dim,), -np.pi, dtype=torch.float32)
-    if max_vals is None:
-        max_vals = torch.full((dim,), np.pi, dtype=torch.float32)
-    return as_tensor(min_vals, torch.float32, device).reshape(dim), as_tensor(max_vals, torch.float32,
-                                                                             device).reshape(dim)
-
-
 def prrtc_plan(
     start_config,
     goal_configs,
@@ -383,11 +374,22 @@ def prrtc_plan(
     step_size, granularity = _validate(step_size, granularity)
     _check_context(collision_context, allow_unsafe_no_collision)
     dev = cuda_device(device)
-    start = as_tensor(start_config, torch.float32, dev).reshape(-1)
-    dim = int(start.shape[0])
-    goals = as_tensor(goal_configs, torch.float32, dev).reshape(-1, dim)
-    lo, hi = _limits(min_vals, max_vals, dim, dev)
-    ctx = DeviceContext(collision_context, dev)
+    # every host input of the call (start, goals, limits, robot and world
+    # tables) goes to the device in one pinned copy, not one blocking pageable
+    # copy per table; tensors already on the device pass through
+    stage = Stager(dev)
+    if isinstance(start_config, torch.Tensor):
+        dim = int(start_config.numel())
+    else:
+        dim = int(np.asarray(start_config).size)
+    k_start = stage.add(start_config, torch.float32, (dim,))
+    k_goals = stage.add(goal_configs, torch.float32, (-1, dim))
+    k_lo = stage.add(np.full(dim, -np.pi, np.float32) if min_vals is None else min_vals, torch.float32, (dim,))
+    k_hi = stage.add(np.full(dim, np.pi, np.float32) if max_vals is None else max_vals, torch.float32, (dim,))
+    ctx = DeviceContext(collision_context, dev, stager=stage)
+    stage.commit()
+    ctx.finish()
+    start, goals, lo, hi = (stage.get(k) for k in (k_start, k_goals, k_lo, k_hi))
 
     inp = _lib.Inputs()
     inp.start_config, inp.goal_configs, inp.num_goals = start.data_ptr(), goals.data_ptr(), goals.shape[0]
