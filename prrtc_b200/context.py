@@ -101,10 +101,12 @@ def build_collision_context(robot: RobotModel, world: dict | None = None) -> dic
     for k, (s, e) in enumerate(zip(starts, ends)):
         locs = sphere_local[s:e].astype(np.float64)
         rads = sphere_radius[s:e].astype(np.float64)
-        c = 0.5 * (locs.min(axis=0) + locs.max(axis=0))
+        # the centre as stored (float32); the reach is measured from it, in
+        # float64, and the radius rounded up, so that the float32 sphere
+        # encloses every fine sphere exactly
+        c = (0.5 * (locs.min(axis=0) + locs.max(axis=0))).astype(np.float32)
         coarse_local[k] = c
-        # round the radius up so the float32 sphere still encloses every fine sphere
-        r = float(np.max(np.linalg.norm(locs - c, axis=1) + rads))
+        r = float(np.max(np.linalg.norm(locs - c.astype(np.float64), axis=1) + rads))
         coarse_radius[k] = np.nextafter(np.float32(r), np.float32(np.inf))
     group_of_frame = {int(f): k for k, f in enumerate(coarse_link)}
 

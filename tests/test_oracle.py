@@ -222,9 +222,11 @@ def test_coarse_model_encloses_fine(arm, dual):
         for k in range(ctx["coarse_sphere_link_idx"].shape[0]):
             s, e = off[k], off[k + 1]
             assert (ctx["sphere_link_idx"][s:e] == ctx["coarse_sphere_link_idx"][k]).all()
-            d = np.linalg.norm(ctx["sphere_local"][s:e] - ctx["coarse_sphere_local"][k], axis=1) + \
-                ctx["sphere_radius"][s:e]
-            assert (d <= ctx["coarse_sphere_radius"][k]).all()
+            # exactly: float64 arithmetic on the stored float32 values
+            d = np.linalg.norm(ctx["sphere_local"][s:e].astype(np.float64) -
+                               ctx["coarse_sphere_local"][k].astype(np.float64), axis=1) + \
+                ctx["sphere_radius"][s:e].astype(np.float64)
+            assert (d <= float(ctx["coarse_sphere_radius"][k])).all()
         rng = ctx["self_pair_ranges"]
         assert rng[0, 0] == 0 and (rng[1:, 0] == rng[:-1, 1]).all() and rng[-1, 1] == ctx["self_pairs"].shape[0]
 
