@@ -378,8 +378,9 @@ static void check_go(const CheckLaunch& o, int full_sweep, const unsigned char* 
 // than PRRTC_CHECK_MINBLOCKS CTAs per SM (large robots: the sphere centres and
 // link frames of a pass grow with S and J); then half or a quarter as many
 // configurations per pass, whichever keeps the most CTAs resident (the larger
-// pass on a tie).  The dual arm with 120 spheres fits one CTA per SM at 32
-// configurations per pass and three at 16: 43.9 -> 60.2 M checks/s.
+// pass on a tie).  The dual arm with 120 spheres and 18 joints fits one CTA
+// per SM at 32 configurations per pass, three at 16 and four at 8: 44.0 M
+// checks/s at 32, 65.4 M at 8.
 cudaError_t launch_check(const unsigned char* blob, int blob_cap, const int32_t* pairs, int J, int S, int K,
                          int Q, int dim, const float* configs, int n, int full_sweep, int32_t* verdicts,
                          cudaStream_t st, const PcView* pc) {
