@@ -14,6 +14,7 @@ from .prrtc import (  # noqa: F401
     prrtc_plan_batch_async,
 )
 from .pointcloud import PointCloud, PointCloudChecker, prrtc_plan_robogpu  # noqa: E402,F401
+from ._lib import PrrtcError, PrrtcTimeout  # noqa: E402,F401
 
 __all__ = [
     "PRRTCResult",
@@ -27,4 +28,6 @@ __all__ = [
     "PointCloud",
     "PointCloudChecker",
     "prrtc_plan_robogpu",
+    "PrrtcError",
+    "PrrtcTimeout",
 ]

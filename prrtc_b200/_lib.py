@@ -6,6 +6,7 @@ it is missing or when no CUDA device is present -- there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import time
 from pathlib import Path
 
 _HERE = Path(__file__).resolve().parent
@@ -180,6 +181,31 @@ def hostpack():
 
 class PrrtcError(RuntimeError):
     pass
+
+
+class PrrtcTimeout(PrrtcError):
+    """A host wait for a call's results ran past its timeout.  The call's work is
+    still queued or running on the GPU; its buffers stay referenced, and the
+    wait can be repeated."""
+
+
+def wait_event(event, timeout_s: float | None, what: str) -> None:
+    """Wait for a CUDA event (an object with ``synchronize()`` and ``query()``):
+    blocking when ``timeout_s`` is None; otherwise polling ``query()``
+    (cudaEventQuery) until the event completes or ``timeout_s`` seconds have
+    passed, then raising PrrtcTimeout.  The poll sleeps 20 us, doubling up to
+    1 ms, so a GPU that stops answering leaves the host with an error instead
+    of a thread blocked for good."""
+    if timeout_s is None:
+        event.synchronize()
+        return
+    deadline = time.monotonic() + max(0.0, float(timeout_s))
+    nap = 20e-6
+    while not event.query():
+        if time.monotonic() >= deadline:
+            raise PrrtcTimeout(f"{what}: not complete after {float(timeout_s):g} s")
+        time.sleep(nap)
+        nap = min(2.0 * nap, 1e-3)
 
 
 def check(rc: int, what: str) -> None:

@@ -242,13 +242,20 @@ class _Results:
         # a private copy: the pinned blocks go back to the allocator's cache now
         return np.concatenate(parts, 0) if len(parts) > 1 else (parts[0].copy() if parts else None)
 
-    def to_results(self, trees: bool = True, paths_on_host: bool = False) -> list[PRRTCResult]:
+    def to_results(self, trees: bool = True, paths_on_host: bool = False,
+                   timeout_s: Optional[float] = None) -> list[PRRTCResult]:
         """One read-back of the [B,16] scalar block (plus, with paths_on_host, one
-        bulk copy of every path) and the per-problem PRRTCResults."""
+        bulk copy of every path) and the per-problem PRRTCResults.  With
+        ``timeout_s``, the wait for the call's kernels polls and raises
+        PrrtcTimeout after that many seconds."""
         if self.ready is not None:
-            self.ready.synchronize()
+            _lib.wait_event(self.ready, timeout_s, "planner results")
             host = self.block_h.numpy().copy()
         else:
+            if timeout_s is not None:
+                done = torch.cuda.Event()
+                done.record()
+                _lib.wait_event(done, timeout_s, "planner results")
             host = self.block.cpu().numpy()
         if (host[:, 8] == -2).any():
             raise _lib.PrrtcError("a device-side wait ran out (scene staging): the planner stopped and these "
@@ -355,11 +362,13 @@ def prrtc_plan(
     threads_per_explorer: int = 0,
     waypoint_chunk: int = 0,
     device=None,
+    timeout_s: Optional[float] = None,
 ) -> PRRTCResult:
     """Plan one problem with the parallel bidirectional RRT-Connect planner (prrtc.py:255-585).
 
     ``jit_trace`` is accepted for signature compatibility; the call is already a
-    single asynchronous C-ABI dispatch.
+    single asynchronous C-ABI dispatch.  ``timeout_s`` bounds the host's wait
+    for the result (PrrtcTimeout after that many seconds; None waits for good).
     """
     collision_mode = _resolve_collision_mode(collision_checker)
     lib = _lib.load()
@@ -410,7 +419,7 @@ def prrtc_plan(
     _lib.check(lib.prrtc_b200_plan(C.byref(inp), C.byref(outs), C.byref(attrs), C.byref(tun), ws.data_ptr(),
                                    ws.numel(), sp), "prrtc_b200_plan")
     res.extract(sp)
-    return res.to_results()[0]
+    return res.to_results(timeout_s=timeout_s)[0]
 
 
 _TABLES = (("world_spheres", 4, np.float32), ("world_capsules", 7, np.float32), ("world_boxes", 15, np.float32),
@@ -766,9 +775,12 @@ class PendingBatch:
         self.res, self.keep, self.stream = res, keep, stream
         self.trees, self.paths_on_host = trees, paths_on_host
 
-    def results(self) -> list[PRRTCResult]:
+    def results(self, timeout_s: Optional[float] = None) -> list[PRRTCResult]:
+        """The batch's results, waiting for its kernels: blocking, or with
+        ``timeout_s`` polling and raising PrrtcTimeout after that many seconds
+        (the batch then stays pending and ``results`` can be called again)."""
         with torch.cuda.stream(self.stream):
-            out = self.res.to_results(trees=self.trees, paths_on_host=self.paths_on_host)
+            out = self.res.to_results(trees=self.trees, paths_on_host=self.paths_on_host, timeout_s=timeout_s)
         self.keep = []
         return out
 
@@ -778,10 +790,12 @@ class PendingBatch:
         return self.res.d2h_bytes
 
 
-def prrtc_plan_batch(start_configs, goal_configs, *args, **kwargs) -> list[PRRTCResult]:
+def prrtc_plan_batch(start_configs, goal_configs, *args, timeout_s: Optional[float] = None,
+                     **kwargs) -> list[PRRTCResult]:
     """Plan B independent problems (prrtc.py:882-1434): the arguments of
-    ``prrtc_plan_batch_async``, waiting for the results."""
-    return prrtc_plan_batch_async(start_configs, goal_configs, *args, **kwargs).results()
+    ``prrtc_plan_batch_async``, waiting for the results (``timeout_s``: see
+    ``PendingBatch.results``)."""
+    return prrtc_plan_batch_async(start_configs, goal_configs, *args, **kwargs).results(timeout_s=timeout_s)
 
 
 def _plan_per_problem(lib, bi, res, attrs, tun, contexts, robot_ctx, starts, goals, goal_counts, lo, hi, dev,
