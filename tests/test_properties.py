@@ -181,6 +181,29 @@ def test_coarse_spheres_enclose_their_fine_spheres_on_random_arms(seed, n_joints
         assert (np.abs(links[:, 0] - links[:, 1]) >= 2).all()
 
 
+@SLOW
+@given(seed=st.integers(0, 10**6), n_joints=st.integers(1, 12))
+def test_self_pair_ranges_are_complete_blocks_of_their_coarse_pairs(seed, n_joints):
+    """Range q of the self-pair list holds exactly the pairs (fine spheres of
+    coarse group a) x (fine spheres of coarse group b) for coarse pair q = (a, b),
+    and the ranges tile the list: the layout the packed checker reads as dense
+    blocks gated by one coarse pair each."""
+    ctx = build_collision_context(scenes.arm(seed, n_joints), None)
+    pairs, cp, rng_ = ctx["self_pairs"], ctx["coarse_self_pairs"], ctx["self_pair_ranges"]
+    off = ctx["fine_link_offsets"]
+    assert cp.shape[0] == rng_.shape[0]
+    cursor = 0
+    for q in range(cp.shape[0]):
+        lo, hi = int(rng_[q, 0]), int(rng_[q, 1])
+        assert lo == cursor and hi >= lo
+        a, b = int(cp[q, 0]), int(cp[q, 1])
+        want = {(i, j) for i in range(off[a], off[a + 1]) for j in range(off[b], off[b + 1])}
+        got = {(int(i), int(j)) for i, j in pairs[lo:hi]}
+        assert got == want and hi - lo == len(want)
+        cursor = hi
+    assert cursor == pairs.shape[0]
+
+
 @FAST
 @given(costs=st.lists(st.floats(0.0, 1e3, allow_nan=False), max_size=300), world=st.integers(1, 8))
 def test_lpt_split_takes_every_problem_once_within_the_list_scheduling_bound(costs, world):
