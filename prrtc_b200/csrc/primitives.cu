@@ -6,6 +6,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "kernels.h"
 #include "prrtc_device.cuh"
@@ -344,6 +345,41 @@ struct CheckLaunch {
     size_t dyn = 0;
 };
 
+// The largest dynamic shared-memory limit set on each check_kernel
+// instantiation, per device and CUDA context.  The limit is only raised, never
+// lowered, so a call on another host thread cannot shrink it between this
+// call's check and its launch, and a call that needs no more than before sets
+// nothing (setting an attribute while an earlier launch runs can make the host
+// wait for that launch).
+struct CheckAttrs {
+    unsigned long long ctx = 0ull;  // context key (current_context_key)
+    int max_dyn = -1;
+};
+constexpr int kCheckAttrDevices = 256;
+static CheckAttrs g_check_attr[kCheckAttrDevices][6];  // [device][2 * (pass size: CW, CW/2, CW/4) + full]
+static std::mutex g_check_attr_mutex;
+
+template <class Kern>
+static cudaError_t check_raise_dyn(Kern kern, int slot, size_t dyn) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long ctx = current_context_key();
+    std::lock_guard<std::mutex> lock(g_check_attr_mutex);
+    CheckAttrs dflt;
+    CheckAttrs& c = (dev >= 0 && dev < kCheckAttrDevices && slot >= 0 && slot < 6) ? g_check_attr[dev][slot] : dflt;
+    if (!ctx || c.ctx != ctx) {
+        c = CheckAttrs{};
+        c.ctx = ctx;
+    }
+    if ((int)dyn > c.max_dyn) {
+        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) != cudaSuccess)
+            return e;
+        c.max_dyn = (int)dyn;
+    }
+    return cudaSuccess;
+}
+
 template <int CW>
 static cudaError_t check_option(int full_sweep, int J, int S, int K, int Q, int blob_cap, CheckLaunch& o) {
     const size_t cc = (size_t)cc_smem_bytes(J, S, K, Q, CW);
@@ -353,7 +389,8 @@ static cudaError_t check_option(int full_sweep, int J, int S, int K, int Q, int 
         dyn = cc;
     }
     auto kern = full_sweep ? check_kernel<CW, true> : check_kernel<CW, false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    constexpr int size_idx = CW == PRRTC_CHECK_CW ? 0 : (2 * CW == PRRTC_CHECK_CW ? 1 : 2);
+    cudaError_t e = check_raise_dyn(kern, 2 * size_idx + (full_sweep ? 1 : 0), dyn);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, dyn)) != cudaSuccess) return e;
