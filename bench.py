@@ -90,7 +90,7 @@ def parse():
                          "smoothing adjoint (smooth) measurement")
     ap.add_argument("--configs", default="1,2,4,5,dense",
                     help="comma list of the extra workloads to measure on rank 0 after the headline: 1 (single plan, "
-                         "GPU and CPU path), 2 (1000 tabletop plans), 4 (smoothing of config-2 paths), 5 (1024 "
+                         "GPU and CPU path), 2 (1000 tabletop plans), 4 (smoothing of the tabletop paths), 5 (1024 "
                          "dual-arm plans + smoothing), dense (the 512-problem batch at the 16-sphere scene's "
                          "density); 'none' skips them")
     ap.add_argument("--split", choices=["weak", "strong"], default="weak",
@@ -1202,10 +1202,10 @@ def measure_config1(torch, dev, n=32, cpu_budget_s=10.0):
 
 
 def measure_config2_4(torch, dev, settings, want4, n=1000, oracle_sample=100, smooth_paths_n=512):
-    """Config 2: n tabletop problems as plain single plans (one launch per
-    problem, 8 streams): success, path cost, device time to solution; the
-    oracle's sequential restatement of the planner on the first problems as the
-    reference.  Config 4: the first 512 solved paths resampled to 64 waypoints,
+    """n tabletop problems as plain single plans (one launch per problem, 8
+    streams): success, path cost, device time to solution; the oracle's
+    sequential restatement of the planner on the first problems as the
+    reference.  Then smoothing: the first 512 solved paths resampled to 64 waypoints,
     50 projected gradient steps of the adjoint cost (each path in its own
     world, one batched launch per step), exact re-validation at 0.01 rad."""
     import multiprocessing as mp
@@ -1305,7 +1305,7 @@ def measure_config4(torch, dev, problems, res, n=512):
     sel = solved[:n]
     paths = [np.asarray(r.path.cpu() if hasattr(r.path, "cpu") else r.path) for _, r in sel]
     out = _smoothing_pass(torch, dev, paths, [p.context for p, _ in sel], sel[0][0].lower, sel[0][0].upper, 64)
-    out["workload"] = f"the first {len(sel)} solved config-2 paths, 64 waypoints x 7 DOF, each in its own world"
+    out["workload"] = f"the first {len(sel)} solved tabletop paths, 64 waypoints x 7 DOF, each in its own world"
     return {"config4_smoothing": out}
 
 

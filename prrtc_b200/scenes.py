@@ -84,7 +84,7 @@ def _straight_pose_clearance(robot: RobotModel) -> float:
 
 
 def arm(seed: int = 0, n_joints: int = 7) -> RobotModel:
-    """Synthetic serial arm (config 1 robot).
+    """Synthetic serial arm (the robot of the single-arm workloads).
 
     Draws robots from seeds ``seed, seed+1000, ...`` and keeps the first whose
     straight pose (q = 0) has every self pair at least 2 cm apart, the same
@@ -125,7 +125,7 @@ def _arm_draw(seed: int, n_joints: int) -> RobotModel:
 
 
 def dual_arm(seed: int = 0) -> RobotModel:
-    """Two config-1 chains 0.6 m apart, each with two mimic finger joints (config 5)."""
+    """Two 7-DOF arm chains 0.6 m apart, each with two mimic finger joints (the dual-arm workload)."""
     single = arm(seed)
     J1 = single.n_joints
     twists, ptf, parent, act, mm, mo, mact = [], [], [], [], [], [], []
