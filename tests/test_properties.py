@@ -6,8 +6,10 @@ index, the nearest-neighbour scan against a float64 argmin over trees with NaN
 slots and duplicate nodes, the extend step and the edge waypoints against their
 geometric definitions, float32 FK against float64 FK on random arms, the
 coarse-gated checkers against the flat checker on random arms and worlds, the
-coarse model's enclosure of its fine spheres, and the longest-processing-time
-split used to shard a batch over ranks.  The draws are derandomized: every run
+coarse model's enclosure of its fine spheres and its self-pair blocks, the
+float64 autograd restatement of the smoothing cost against the C oracle's cost
+and its central differences, and the longest-processing-time split used to
+shard a batch over ranks.  The draws are derandomized: every run
 tests the same examples.
 """
 from __future__ import annotations
@@ -202,6 +204,38 @@ def test_self_pair_ranges_are_complete_blocks_of_their_coarse_pairs(seed, n_join
         assert got == want and hi - lo == len(want)
         cursor = hi
     assert cursor == pairs.shape[0]
+
+
+@SLOW
+@given(seed=st.integers(0, 10**6), n_joints=st.integers(2, 9), wseed=seeds,
+       kind=st.sampled_from(["spheres", "tabletop", "uneven"]), n_wp=st.integers(3, 8),
+       margin=st.sampled_from([0.0, 0.02, 0.05]), beta=st.sampled_from([20.0, 50.0]))
+def test_autodiff_smoothing_cost_matches_the_oracle_on_random_arms_worlds_and_paths(orc, seed, n_joints, wseed,
+                                                                                    kind, n_wp, margin, beta):
+    """The float64 autograd restatement of the smoothing cost -- the reference
+    the GPU adjoint is checked against -- equals the C oracle's cost, and its
+    gradient equals central differences of that cost."""
+    from oracle.smooth_autodiff import smooth_grad
+
+    robot = scenes.arm(seed, n_joints)
+    rng = np.random.default_rng(wseed)
+    world = {"spheres": lambda: scenes.spheres_world(rng, 16), "tabletop": lambda: scenes.tabletop_world(rng),
+             "uneven": lambda: scenes.uneven_world(rng)}[kind]()
+    ctx = build_collision_context(robot, world)
+    sc = orc.Scene(ctx, robot.dim)
+    ends = rng.uniform(robot.lower, robot.upper, (2, robot.dim))
+    w = np.linspace(ends[0], ends[1], n_wp) + rng.normal(0, 0.05, (n_wp, robot.dim))
+    c, g = smooth_grad(ctx, w, margin, beta, 1.0)
+    c64 = sc.smooth_cost(w, margin, beta, 1.0)
+    assert abs(c - c64) <= 1e-9 * max(1.0, abs(c64))
+    h = 1e-5
+    for _ in range(4):
+        i, d = int(rng.integers(0, n_wp)), int(rng.integers(0, robot.dim))
+        wp, wm = w.copy(), w.copy()
+        wp[i, d] += h
+        wm[i, d] -= h
+        fd = (sc.smooth_cost(wp, margin, beta, 1.0) - sc.smooth_cost(wm, margin, beta, 1.0)) / (2 * h)
+        assert abs(g[i, d] - fd) <= 1e-5 * max(1.0, abs(fd)), (i, d, g[i, d], fd)
 
 
 @FAST
