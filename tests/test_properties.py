@@ -8,8 +8,9 @@ geometric definitions, float32 FK against float64 FK on random arms, the
 coarse-gated checkers against the flat checker on random arms and worlds, the
 coarse model's enclosure of its fine spheres and its self-pair blocks, the
 float64 autograd restatement of the smoothing cost against the C oracle's cost
-and its central differences, and the longest-processing-time split used to
-shard a batch over ranks.  The draws are derandomized: every run
+and its central differences, the paths of the two CPU planners (the
+sequential restatement and the host-driven loop of the CPU baseline), and the
+longest-processing-time split used to shard a batch over ranks.  The draws are derandomized: every run
 tests the same examples.
 """
 from __future__ import annotations
@@ -236,6 +237,51 @@ def test_autodiff_smoothing_cost_matches_the_oracle_on_random_arms_worlds_and_pa
         wm[i, d] -= h
         fd = (sc.smooth_cost(wp, margin, beta, 1.0) - sc.smooth_cost(wm, margin, beta, 1.0)) / (2 * h)
         assert abs(g[i, d] - fd) <= 1e-5 * max(1.0, abs(fd)), (i, d, g[i, d], fd)
+
+
+PLANS = settings(max_examples=12, deadline=None, derandomize=True)
+
+
+@PLANS
+@given(kind=st.sampled_from(["spheres16", "tabletop", "uneven"]), seed=st.integers(0, 10**6))
+def test_oracle_planner_paths_join_start_to_goal_and_revalidate(orc, kind, seed):
+    """Whenever the sequential restatement of the planner solves a random
+    problem, its path runs from the start to one of the goals and re-validates
+    at 0.01 rad under the rules the GPU planner's paths are held to."""
+    from conftest import make_problem
+
+    pr = make_problem(kind, seed)
+    sc = orc.Scene(pr.context, pr.dim)
+    r = orc.plan(sc, pr.start, pr.goals, pr.lower, pr.upper, max_iterations=1000, num_new_samples=16,
+                 max_nodes=pr.max_nodes, collision_mode=3, edge_resolution=0.01)
+    if r.solved != 1:
+        assert r.path is None
+        return
+    assert np.array_equal(r.path[0], pr.start) and any(np.array_equal(r.path[-1], g) for g in pr.goals)
+    ok, md = sc.validate_planned_path(r.path, 16, 0.01)
+    assert ok, md
+
+
+@PLANS
+@given(kind=st.sampled_from(["spheres16", "tabletop", "uneven"]), seed=st.integers(0, 10**6),
+       rseed=st.integers(0, 2**31 - 1))
+def test_host_loop_paths_are_free_on_their_own_edge_waypoints(orc, kind, seed, rseed):
+    """Whenever the host-driven loop (the CPU baseline) solves a random problem,
+    its path runs from the start to the goal, and every vertex and every one of
+    the 16 waypoints per edge it checked is free (within 1e-5 m: float32
+    against float64)."""
+    from conftest import make_problem
+
+    pr = make_problem(kind, seed)
+    sc = orc.Scene(pr.context, pr.dim)
+    r = orc.rrtc_host_plan(sc, pr.start, pr.goals[0], pr.lower, pr.upper, max_iterations=300,
+                           num_new_samples=32, seed=rseed)
+    if not r.solved:
+        return
+    p = r.path
+    assert np.array_equal(p[0], pr.start) and np.array_equal(p[-1], pr.goals[0])
+    pts = np.concatenate([p] + [orc.edge_waypoints(p[i], p[i + 1], 16, 0.0) for i in range(p.shape[0] - 1)])
+    assert sc.min_distances(pts).min() >= -1e-5
 
 
 @FAST
